@@ -1,0 +1,118 @@
+// Decoder context set-up.  See context.h.
+#include "context.h"
+
+#include <stdio.h>
+#include <sys/stat.h>
+
+namespace dvc {
+
+bool DevBuf::ensure(size_t b) {
+  if (b <= bytes && p) return true;
+  release();
+  if (cudaMalloc(&p, b ? b : 16) != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    return false;
+  }
+  bytes = b;
+  return true;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+bool Context::cuda_ok(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return true;
+  err = std::string(what) + ": " + cudaGetErrorString(e);
+  return false;
+}
+
+static bool file_exists(const std::string &p) {
+  struct stat st;
+  return stat(p.c_str(), &st) == 0;
+}
+
+bool Context::init(const char *data, const char *tables, int dev) {
+  device = dev;
+  data_dir = data ? data : "";
+  table_dir = tables ? tables : data_dir;
+  mkdir(table_dir.c_str(), 0755);
+  if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return false;
+  if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+
+  // library-exact math tables: load, or sweep the C library once and cache
+  const std::string xpath = table_dir + "/xlm_tables.bin";
+  char ebuf[256] = {0};
+  if (dvc_libm_load(xpath.c_str(), &xlm_host, ebuf, sizeof ebuf) != 0) {
+    fprintf(stderr, "dvc_b200: building C-library correction tables (%s)\n", ebuf);
+    if (dvc_libm_build(xpath.c_str(), 0, ebuf, sizeof ebuf) != 0) return fail(std::string("libm table build: ") + ebuf);
+    if (dvc_libm_load(xpath.c_str(), &xlm_host, ebuf, sizeof ebuf) != 0) return fail(std::string("libm table load: ") + ebuf);
+  }
+  auto up = [&](const std::vector<uint32_t> &v, const uint32_t **dst) {
+    void *p = nullptr;
+    if (cudaMalloc(&p, v.size() * 4) != cudaSuccess) return false;
+    xlm_allocs.push_back(p);
+    if (cudaMemcpy(p, v.data(), v.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) return false;
+    *dst = (const uint32_t *)p;
+    return true;
+  };
+  if (!up(xlm_host.log_tab, &xlm.log_tab) || !up(xlm_host.exp_tab, &xlm.exp_tab) ||
+      !up(xlm_host.em1_bitmap, &xlm.em1_bitmap))
+    return fail("uploading libm tables failed");
+  auto lg2 = [](uint32_t v) {
+    int s = 0;
+    while ((1u << s) < v) s++;
+    return s;
+  };
+  xlm.log_mask = xlm_host.hdr.log_cap - 1;
+  xlm.exp_mask = xlm_host.hdr.exp_cap - 1;
+  xlm.log_shift = 32 - lg2(xlm_host.hdr.log_cap);
+  xlm.exp_shift = 32 - lg2(xlm_host.hdr.exp_cap);
+  xlm.tanh_ylo = xlm_host.hdr.tanh_ylo;
+  xlm.tanh_y1 = xlm_host.hdr.tanh_y1;
+
+  // LDPCA ladders (QCIF n=1584 and CIF n=6336)
+  const std::string lpath = data_dir + "/ldpca_ladders.bin";
+  if (!file_exists(lpath)) return fail("missing ladder file " + lpath);
+  if (!load_ladders(lpath, ladders_host, err)) return false;
+  ladders_gpu.resize(ladders_host.size());
+  for (size_t i = 0; i < ladders_host.size(); i++) {
+    LadderHost &L = ladders_host[i];
+    const std::string cache = table_dir + "/invh_" + std::to_string(L.n) + ".bin";
+    if (!ladder_inverse(L, cache, err)) return false;
+    if (!ladders_gpu[i].upload(L, err)) return false;
+  }
+  return true;
+}
+
+void Context::release() {
+  for (auto &g : ladders_gpu) g.release();
+  ladders_gpu.clear();
+  for (void *p : xlm_allocs) cudaFree(p);
+  xlm_allocs.clear();
+  ld_lr.release();
+  ld_acc.release();
+  ld_dec.release();
+  ld_res.release();
+  ld_ent.release();
+  ld_jobs.release();
+  if (stream) cudaStreamDestroy(stream);
+  stream = nullptr;
+}
+
+const LadderDev *Context::ladder(int n) const {
+  for (size_t i = 0; i < ladders_host.size(); i++)
+    if (ladders_host[i].n == n) return &ladders_gpu[i].dev;
+  return nullptr;
+}
+
+const LadderHost *Context::ladder_host(int n) const {
+  for (auto &L : ladders_host)
+    if (L.n == n) return &L;
+  return nullptr;
+}
+
+}  // namespace dvc

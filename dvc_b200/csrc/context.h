@@ -1,0 +1,48 @@
+// Per-device decoder context: library-exact math tables, LDPCA ladders,
+// streams and reusable device buffers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "dvc_types.h"
+#include "ladder.h"
+#include "libm_tables.h"
+
+namespace dvc {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  bool ensure(size_t b);
+  void release();
+  template <class T>
+  T *as() const { return (T *)p; }
+};
+
+struct Context {
+  int device = 0;
+  std::string data_dir, table_dir;
+  std::string err;
+  XlmHost xlm_host;
+  XlmDev xlm{};
+  std::vector<void *> xlm_allocs;
+  std::vector<LadderHost> ladders_host;
+  std::vector<LadderGpu> ladders_gpu;
+  cudaStream_t stream = nullptr;
+  // scratch for the batched LDPCA entry point
+  DevBuf ld_lr, ld_acc, ld_dec, ld_res, ld_ent, ld_jobs;
+
+  bool init(const char *data_dir, const char *table_dir, int device);
+  void release();
+  const LadderDev *ladder(int n) const;
+  const LadderHost *ladder_host(int n) const;
+  bool fail(const std::string &m) {
+    err = m;
+    return false;
+  }
+  bool cuda_ok(cudaError_t e, const char *what);
+};
+
+}  // namespace dvc

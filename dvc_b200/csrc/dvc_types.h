@@ -1,0 +1,47 @@
+// Plain-data structures shared by the host driver and the kernels.
+#pragma once
+#include <stdint.h>
+
+namespace dvc {
+
+// LDPCA ladder for one codeword length, resident in device memory.
+// Derived from the reference's ladder tables (ReadLdpcaLadderFile_LdpcaDecoder.cpp:150-201):
+// per code c the syndrome length m_c = (n/period)*bpp[c], its rate m_c/n, the
+// row of every edge ir_c[e], plus layouts this decoder adds for parallel BP:
+// per code the edges of each row in increasing edge order (row_ptr/row_edge,
+// so that row sums keep the reference's summation order), the column of every
+// edge, the CRC-8 contribution of each single source bit, and the GF(2)
+// inverse of the full-rate matrix with bit i of row j at word i/32, bit i%32.
+struct LadderDev {
+  int n, e, period, num_codes, invh_words;
+  const int *jc;          // [n+1]
+  const int *bpp;         // [num_codes]
+  const int *idx;         // [num_codes*period]
+  const int *synd_len;    // [num_codes]
+  const float *code_rate; // [num_codes]
+  const int *row_ptr;     // [num_codes*(n+1)]
+  const uint16_t *row_edge;  // [num_codes*e]
+  const uint16_t *ir;        // [num_codes*e]
+  const uint16_t *edge_col;  // [e]
+  const uint8_t *crc_tab;    // [n]
+  const uint32_t *invh;      // [n*invh_words]
+};
+
+// One LDPCA decode request: a bitplane of one WZ frame.
+struct LdpcaJob {
+  const float *lr;       // [n] p0/p1 per 4x4 block (condBitProb output)
+  const uint8_t *acc;    // [n/8] accumulated syndrome bytes, MSB first
+  int crc;               // CRC-8 of the source bitplane
+  uint8_t *decoded;      // [n] decoded bits (may be null)
+  int *result;           // [4] rate (m+8), first code tried, accepted code, BP iterations run
+  float *entropy;        // conditional entropy bound (may be null)
+  int use_given_entropy; // 1: take the bound from given_entropy instead of computing it
+  float given_entropy;
+  float *llr_out;        // [n] log(p0/p1) written back (may alias lr), or null
+  // optional fused putBitplaneToCoeff (bitplane.cpp:4-22)
+  int *recons_trans;     // [w*h] quantisation indices, or null
+  const uint8_t *mode;   // [w*h/64] block modes
+  int w, index_in_blk;
+};
+
+}  // namespace dvc

@@ -1,0 +1,129 @@
+"""ctypes binding of libdvc_b200.so (the C ABI in include/dvc_b200.h).
+
+The library is built in-tree by ``dvc_b200.build``; importing this module does
+not build it.  A missing library or a failing CUDA set-up raises immediately:
+there is no CPU fallback.
+"""
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libdvc_b200.so")
+DATA_DIR = os.path.join(HERE, "ladders")
+TABLE_DIR = os.environ.get("DVC_B200_TABLES", os.path.join(HERE, "_tables"))
+
+DVC_OK, DVC_E_ARG, DVC_E_CUDA, DVC_E_NOMEM, DVC_E_DATA = 0, -1, -2, -3, -4
+
+
+class DvcError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("dvc_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise FileNotFoundError("libdvc_b200.so not built (%s); run python -m dvc_b200.build" % LIB_PATH)
+            L = C.CDLL(LIB_PATH)
+            L.dvc_create.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+            L.dvc_create.restype = C.c_int
+            L.dvc_destroy.argtypes = [C.c_void_p]
+            L.dvc_destroy.restype = None
+            L.dvc_last_error.argtypes = [C.c_void_p]
+            L.dvc_last_error.restype = C.c_char_p
+            L.dvc_ldpca_decode.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+            L.dvc_ldpca_decode.restype = C.c_int
+            L.dvc_LdpcaDecoder.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.POINTER(C.c_int), C.c_ubyte, C.c_float]
+            L.dvc_LdpcaDecoder.restype = C.c_int
+            _declare_frame_api(L)
+            _lib = L
+    return _lib
+
+
+def _declare_frame_api(L):
+    """Declarations of the frame-level entry points (present once built)."""
+    for name, args in FRAME_API.items():
+        if hasattr(L, name):
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+
+
+FRAME_API = {}
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """A decoder context on one CUDA device (dvc_create / dvc_destroy)."""
+
+    def __init__(self, device=0, table_dir=None):
+        self._h = C.c_void_p()
+        td = table_dir or TABLE_DIR
+        os.makedirs(td, exist_ok=True)
+        rc = lib().dvc_create(DATA_DIR.encode(), td.encode(), device, C.byref(self._h))
+        if rc != DVC_OK:
+            msg = lib().dvc_last_error(self._h).decode() if self._h else "create failed"
+            if self._h:
+                lib().dvc_destroy(self._h)
+                self._h = C.c_void_p()
+            raise DvcError(rc, msg)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, rc):
+        if rc != DVC_OK:
+            raise DvcError(rc, lib().dvc_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            lib().dvc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def ldpca_decode(self, lr, acc_bytes, crc, max_iter=50):
+        """Batched LDPCA decode. lr: (count, n) float32 p0/p1; acc_bytes: (count, n/8) uint8;
+        crc: (count,) uint8. Returns (decoded (count, n) uint8, results (count, 4) int32, entropy (count,))."""
+        lr = np.ascontiguousarray(lr, np.float32)
+        if lr.ndim == 1:
+            lr = lr[None]
+        count, n = lr.shape
+        acc = np.ascontiguousarray(acc_bytes, np.uint8).reshape(count, n // 8)
+        crc = np.ascontiguousarray(crc, np.uint8).reshape(count)
+        dec = np.zeros((count, n), np.uint8)
+        res = np.zeros((count, 4), np.int32)
+        ent = np.zeros(count, np.float32)
+        self.check(lib().dvc_ldpca_decode(self._h, n, count, _ptr(lr), _ptr(acc), _ptr(crc), _ptr(dec), _ptr(res),
+                                          _ptr(ent), max_iter))
+        return dec, res, ent
+
+    def LdpcaDecoder(self, lr, acc_bits, crc, rate_lower_bound):
+        """Reference-shaped call: returns (decoded bits, rate, log LR)."""
+        lr = np.ascontiguousarray(lr, np.float32).copy()
+        acc = np.ascontiguousarray(acc_bits, np.uint8)
+        dec = np.zeros(len(lr), np.uint8)
+        rate = C.c_int(0)
+        self.check(lib().dvc_LdpcaDecoder(self._h, len(lr), _ptr(lr), _ptr(acc), _ptr(dec), C.byref(rate),
+                                          C.c_ubyte(int(crc)), C.c_float(rate_lower_bound)))
+        return dec, rate.value, lr
