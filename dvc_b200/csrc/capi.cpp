@@ -6,12 +6,23 @@
 #include <new>
 #include <vector>
 
+#include <map>
+
 #include "context.h"
+#include "frame_driver.h"
 #include "kernels.h"
 
 struct dvc_ctx {
   dvc::Context c;
+  dvc::FrameBatcher batcher;
+  // device copies of host frames handed to dvc_decode_wz_frames
+  std::vector<dvc::DevBuf> ref, lp, ip, out, dbf;
+  dvc::DevBuf dbg;
 };
+
+namespace dvc {
+cudaError_t launch_ref_planes(const uint8_t *recon, int w, int h, uint8_t *lp, uint8_t *ip, cudaStream_t s);
+}
 
 using dvc::Context;
 
@@ -38,6 +49,10 @@ extern "C" int dvc_create(const char *data_dir, const char *table_dir, int devic
 
 extern "C" void dvc_destroy(dvc_ctx *ctx) {
   if (!ctx) return;
+  ctx->batcher.release();
+  for (auto *v : {&ctx->ref, &ctx->lp, &ctx->ip, &ctx->out, &ctx->dbf})
+    for (auto &b : *v) b.release();
+  ctx->dbg.release();
   ctx->c.release();
   delete ctx;
 }
@@ -67,6 +82,7 @@ static int ldpca_run(Context &c, int n, int count, const float *lr, const uint8_
   for (int i = 0; i < count; i++) {
     dvc::LdpcaJob &j = jobs[i];
     memset(&j, 0, sizeof j);
+    j.active = 1;
     j.lr = c.ld_lr.as<float>() + (size_t)i * n;
     j.acc = c.ld_acc.as<uint8_t>() + (size_t)i * nb;
     j.crc = crc[i];
@@ -126,5 +142,142 @@ extern "C" int dvc_LdpcaDecoder(dvc_ctx *ctx, int n, float *LR_intrinsic, const 
                      LR_intrinsic);
   if (st != DVC_OK) return st;
   *rate = res[0];
+  return DVC_OK;
+}
+
+static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t *dbg_si0, float *dbg_alpha,
+                         uint8_t *dbg_si1);
+
+extern "C" int dvc_decode_wz_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames) {
+  return decode_frames(ctx, count, frames, nullptr, nullptr, nullptr);
+}
+
+extern "C" int dvc_debug_wz_frame(dvc_ctx *ctx, dvc_wz_frame *frame, uint8_t *si_initial, float *alpha,
+                                  uint8_t *si_final) {
+  return decode_frames(ctx, 1, frame, si_initial, alpha, si_final);
+}
+
+static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t *dbg_si0, float *dbg_alpha,
+                         uint8_t *dbg_si1) {
+  if (!ctx) return DVC_E_ARG;
+  Context &c = ctx->c;
+  if (count <= 0 || !frames) {
+    c.err = "dvc_decode_wz_frames: no frames";
+    return DVC_E_ARG;
+  }
+  const int w = frames[0].width, h = frames[0].height;
+  for (int i = 0; i < count; i++) {
+    const dvc_wz_frame &f = frames[i];
+    if (f.width != w || f.height != h || !((w == 176 && h == 144) || (w == 352 && h == 288))) {
+      c.err = "frames must all be QCIF (176x144) or all CIF (352x288)";
+      return DVC_E_ARG;
+    }
+    if (f.qindex < 1 || f.qindex > 8 || !f.past || !f.future || !f.ac_range || !f.crc || !f.acc_synd || !f.recon) {
+      c.err = "dvc_decode_wz_frames: bad frame " + std::to_string(i);
+      return DVC_E_ARG;
+    }
+  }
+  const size_t fs = (size_t)w * h;
+  cudaStream_t s = c.stream;
+  // distinct reference frames (by host pointer), each uploaded once with its planes
+  std::map<const uint8_t *, int> refs;
+  for (int i = 0; i < count; i++)
+    for (const uint8_t *p : {frames[i].past, frames[i].future})
+      if (!refs.count(p)) {
+        const int k = (int)refs.size();
+        refs[p] = k;
+      }
+  const size_t nr = refs.size();
+  if (ctx->ref.size() < nr) {
+    ctx->ref.resize(nr);
+    ctx->lp.resize(nr);
+    ctx->ip.resize(nr);
+  }
+  if (ctx->out.size() < (size_t)count) {
+    ctx->out.resize(count);
+    ctx->dbf.resize(count);
+  }
+  int st;
+  for (auto &kv : refs) {
+    const int k = kv.second;
+    if (!ctx->ref[k].ensure(fs) || !ctx->lp[k].ensure(fs) || !ctx->ip[k].ensure(fs * 4)) {
+      c.err = "device allocation failed";
+      return DVC_E_NOMEM;
+    }
+    if ((st = cuda_status(c, cudaMemcpyAsync(ctx->ref[k].p, kv.first, fs, cudaMemcpyHostToDevice, s), "H2D ref")))
+      return st;
+    if ((st = cuda_status(c, dvc::launch_ref_planes(ctx->ref[k].as<uint8_t>(), w, h, ctx->lp[k].as<uint8_t>(),
+                                                    ctx->ip[k].as<uint8_t>(), s),
+                          "reference planes")))
+      return st;
+  }
+  std::vector<dvc::FrameSpec> specs(count);
+  for (int i = 0; i < count; i++) {
+    const dvc_wz_frame &f = frames[i];
+    if (!ctx->out[i].ensure(fs) || !ctx->dbf[i].ensure(fs)) {
+      c.err = "device allocation failed";
+      return DVC_E_NOMEM;
+    }
+    if ((st = cuda_status(c, cudaMemcpyAsync(ctx->out[i].p, f.recon, fs, cudaMemcpyHostToDevice, s), "H2D recon")))
+      return st;
+    dvc::FrameSpec &S = specs[i];
+    S.w = w;
+    S.h = h;
+    S.qindex = f.qindex;
+    const int pr = refs[f.past], fr = refs[f.future];
+    S.past = ctx->ref[pr].as<uint8_t>();
+    S.future = ctx->ref[fr].as<uint8_t>();
+    S.past_lp = ctx->lp[pr].as<uint8_t>();
+    S.future_lp = ctx->lp[fr].as<uint8_t>();
+    S.past_ip = ctx->ip[pr].as<uint8_t>();
+    S.future_ip = ctx->ip[fr].as<uint8_t>();
+    S.past_idx = f.past_idx;
+    S.future_idx = f.future_idx;
+    S.cur_idx = f.cur_idx;
+    S.mode = f.mode;
+    S.skip_mode = f.skip_mode;
+    S.intra_mode = f.intra_mode;
+    for (int j = 0; j < 16; j++) S.ac_range[j] = f.ac_range[j];
+    S.crc = f.crc;
+    S.acc = f.acc_synd;
+    S.recon = ctx->out[i].as<uint8_t>();
+    S.deblock_flag = ctx->dbf[i].as<uint8_t>();
+  }
+  dvc::DevBuf &dbg = ctx->dbg;
+  if (dbg_si0 || dbg_alpha || dbg_si1) {
+    if (!dbg.ensure(fs * 6)) {
+      c.err = "device allocation failed";
+      return DVC_E_NOMEM;
+    }
+    specs[0].dbg_si_initial = dbg.as<uint8_t>();
+    specs[0].dbg_si_final = dbg.as<uint8_t>() + fs;
+    specs[0].dbg_alpha = (float *)(dbg.as<uint8_t>() + 2 * fs);
+  }
+  std::vector<dvc::FrameResult> res;
+  if (!ctx->batcher.decode(c, specs, res, s)) return c.err.find("alloc") != std::string::npos ? DVC_E_NOMEM : DVC_E_CUDA;
+  for (int i = 0; i < count; i++) {
+    dvc_wz_frame &f = frames[i];
+    if ((st = cuda_status(c, cudaMemcpyAsync(f.recon, ctx->out[i].p, fs, cudaMemcpyDeviceToHost, s), "D2H recon")))
+      return st;
+    if (f.deblock_flag &&
+        (st = cuda_status(c, cudaMemcpyAsync(f.deblock_flag, ctx->dbf[i].p, fs, cudaMemcpyDeviceToHost, s), "D2H dbf")))
+      return st;
+  }
+  if (dbg_si0 && (st = cuda_status(c, cudaMemcpyAsync(dbg_si0, dbg.p, fs, cudaMemcpyDeviceToHost, s), "D2H dbg")))
+    return st;
+  if (dbg_si1 &&
+      (st = cuda_status(c, cudaMemcpyAsync(dbg_si1, dbg.as<uint8_t>() + fs, fs, cudaMemcpyDeviceToHost, s), "D2H dbg")))
+    return st;
+  if (dbg_alpha &&
+      (st = cuda_status(c, cudaMemcpyAsync(dbg_alpha, dbg.as<uint8_t>() + 2 * fs, fs * 4, cudaMemcpyDeviceToHost, s),
+                        "D2H dbg")))
+    return st;
+  if ((st = cuda_status(c, cudaStreamSynchronize(s), "decode sync"))) return st;
+  for (int i = 0; i < count; i++) {
+    dvc_wz_frame &f = frames[i];
+    f.wz_bits = res[i].wz_bits;
+    if (f.plane_results) memcpy(f.plane_results, res[i].planes.data(), res[i].planes.size() * sizeof(int));
+    if (f.plane_entropy) memcpy(f.plane_entropy, res[i].entropy.data(), res[i].entropy.size() * sizeof(float));
+  }
   return DVC_OK;
 }

@@ -29,6 +29,7 @@ struct LadderDev {
 
 // One LDPCA decode request: a bitplane of one WZ frame.
 struct LdpcaJob {
+  int active;            // 0: the block returns at once (frame not in this step)
   const float *lr;       // [n] p0/p1 per 4x4 block (condBitProb output)
   const uint8_t *acc;    // [n/8] accumulated syndrome bytes, MSB first
   int crc;               // CRC-8 of the source bitplane

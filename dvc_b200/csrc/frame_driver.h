@@ -1,0 +1,71 @@
+// Host driver of batched WZ-frame decoding on the device.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "frame_types.h"
+
+namespace dvc {
+
+// quantiser tables and derived per-frame constants (reconstruction.cpp:9-78,
+// wzbitstream.cpp:165-175, DVC_Decoder.cpp:139-152)
+extern const int kQTable[9][16];
+extern const int kQBits[9][16];
+extern const int kZigzag[16];
+int qbits_per_block(int q);
+
+// One WZ frame of a batch.  Reference frames and the output live on the device.
+struct FrameSpec {
+  int w = 0, h = 0, qindex = 0;
+  const uint8_t *past = nullptr, *future = nullptr;        // device [w*h]
+  const uint8_t *past_lp = nullptr, *future_lp = nullptr;  // device [w*h]
+  const uint8_t *past_ip = nullptr, *future_ip = nullptr;  // device [4*w*h]
+  int past_idx = 0, future_idx = 0, cur_idx = 0;
+  const uint8_t *mode = nullptr;  // host [w*h/64], null = every block WZ
+  int skip_mode = 0, intra_mode = 0;
+  int ac_range[16] = {0};
+  const uint8_t *crc = nullptr;   // host [qbits]
+  const uint8_t *acc = nullptr;   // host [qbits*w*h/128]
+  uint8_t *recon = nullptr;       // device [w*h]; intra blocks filled in by the caller
+  uint8_t *deblock_flag = nullptr;  // device [w*h] out, or null
+  // optional device copies of intermediate stages (stage-level parity checks)
+  uint8_t *dbg_si_initial = nullptr;  // side information after createSideInfo + intra copy
+  float *dbg_alpha = nullptr;         // noise parameters
+  uint8_t *dbg_si_final = nullptr;    // side information after the last refinement
+};
+
+struct FrameResult {
+  int wz_bits = 0;                // 10 per coded AC band + sum over bitplanes of (m+8)
+  std::vector<int> planes;        // per bitplane: rate, first code, accepted code, BP iterations
+  std::vector<float> entropy;     // per bitplane conditional-entropy bound
+};
+
+struct Slot {
+  int w = 0, h = 0;
+  DevBuf si, dbf, residue, side_trans, recons_trans, alpha, lr, oct, smf, pdf;
+  DevBuf mb_mv, fmv, blk_mv, blk_mv2, holes, mse, stats, in, out;
+  bool ensure(int w, int h, size_t pdf_floats, size_t in_bytes, size_t out_bytes);
+  void release();
+};
+
+class FrameBatcher {
+ public:
+  bool decode(Context &ctx, const std::vector<FrameSpec> &frames, std::vector<FrameResult> &results,
+              cudaStream_t stream, int max_iter = 50);
+  void release();
+  size_t slots() const { return slots_.size(); }
+
+ private:
+  std::vector<Slot> slots_;
+  DevBuf frames_dev_, jobs_dev_;
+  std::vector<uint8_t> staging_;
+  void *pinned_ = nullptr;
+  size_t pinned_bytes_ = 0;
+  bool ensure_pinned(size_t b);
+};
+
+}  // namespace dvc

@@ -1,0 +1,1004 @@
+// Wyner-Ziv frame kernels other than LDPCA: side-information creation,
+// transforms, correlation-noise model, conditional bit probabilities,
+// reconstruction, side-information refinement and motion learning.
+//
+// Every kernel takes the array of per-frame descriptors of a batch and uses
+// blockIdx.y (or blockIdx.x for single-block-per-frame kernels) as the frame
+// index, so one launch serves every frame of the batch.  Frames whose
+// descriptor is not `active` return at once.
+//
+// Each kernel restates one reference function (paths in DvcDec/src) with the
+// same operation order for every float/double result; the module is compiled
+// with -fmad=false so no multiply-add is fused.
+#include <cuda_runtime.h>
+
+#include "dvc_common.cuh"
+#include "frame_types.h"
+#include "kernels.h"
+
+namespace dvc {
+
+#define SEARCH_R 32  // defines.h:8
+#define LEARN_R 4    // defines.h:11
+#define ML_N 81
+
+__constant__ double c_post_scale[16];
+__constant__ double c_pre_scale[16];
+
+cudaError_t upload_transform_scales(const double *post, const double *pre) {
+  cudaError_t e = cudaMemcpyToSymbol(c_post_scale, post, sizeof(double) * 16);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(c_pre_scale, pre, sizeof(double) * 16);
+}
+
+// Does the frame take part in step (band, bit)?  band < 0: frame-level steps.
+// Bands are decoded in zig-zag order while Qbits > 0 (DVC_Decoder.cpp:161-165,
+// 403-407); bitplanes from Qbits down to 1 (:196).
+__device__ __forceinline__ bool in_step(const FrameDev &F, int band, int bit) {
+  if (band < 0) return true;
+  for (int b = 0; b <= band; b++)
+    if (F.qbits[c_zigzag[b]] <= 0) return false;
+  return bit <= 0 || bit <= F.qbits[c_zigzag[band]];
+}
+
+// ROUND, defines.h:23
+__device__ __forceinline__ int dround(double x) { return x >= 0.0 ? (int)(x + 0.5) : -(int)(-x + 0.5); }
+
+// costFunc, sideInfoCreation.cpp:10-12 (K is the float 0.05f, promoted)
+__device__ __forceinline__ double cost_func(double mad, double vx, double vy) {
+  return mad * (1.0 + (double)0.05f * sqrt(vx * vx + vy * vy));
+}
+
+// computeEndPoint, sideInfoCreation.cpp:14-22
+__device__ __forceinline__ int end_point(double st, double v, double scale, int lo, int hi) {
+  const int e = (int)((st + v * scale) + 0.5);
+  return e < lo ? lo : (e > hi ? hi : e);
+}
+
+// forward44, transform.cpp:63-104
+__device__ __forceinline__ void forward44(int *blk) {
+  int t[16];
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    t[c] = blk[c] + blk[4 + c] + blk[8 + c] + blk[12 + c];
+    t[4 + c] = (blk[c] << 1) + blk[4 + c] - blk[8 + c] - (blk[12 + c] << 1);
+    t[8 + c] = blk[c] - blk[4 + c] - blk[8 + c] + blk[12 + c];
+    t[12 + c] = blk[c] - (blk[4 + c] << 1) + (blk[8 + c] << 1) - blk[12 + c];
+  }
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int *s = t + 4 * r;
+    int *o = blk + 4 * r;
+    o[0] = s[0] + s[1] + s[2] + s[3];
+    o[1] = (s[0] << 1) + s[1] - s[2] - (s[3] << 1);
+    o[2] = s[0] - s[1] - s[2] + s[3];
+    o[3] = s[0] - (s[1] << 1) + (s[2] << 1) - s[3];
+  }
+#pragma unroll
+  for (int i = 0; i < 16; i++) blk[i] = dround(((double)blk[i]) * c_post_scale[i]);
+}
+
+// inverse44, transform.cpp:106-151
+__device__ __forceinline__ void inverse44(int *blk) {
+  int t[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) blk[i] = dround(((double)blk[i]) * c_pre_scale[i]);
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    t[c] = blk[c] + blk[4 + c] + blk[8 + c] + (blk[12 + c] >> 1);
+    t[4 + c] = blk[c] + (blk[4 + c] >> 1) - blk[8 + c] - blk[12 + c];
+    t[8 + c] = blk[c] - (blk[4 + c] >> 1) - blk[8 + c] + blk[12 + c];
+    t[12 + c] = blk[c] - blk[4 + c] + blk[8 + c] - (blk[12 + c] >> 1);
+  }
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int *s = t + 4 * r;
+    int *o = blk + 4 * r;
+    o[0] = s[0] + s[1] + s[2] + (s[3] >> 1);
+    o[1] = s[0] + (s[1] >> 1) - s[2] - s[3];
+    o[2] = s[0] - (s[1] >> 1) - s[2] + s[3];
+    o[3] = s[0] - s[1] + s[2] - (s[3] >> 1);
+  }
+#pragma unroll
+  for (int i = 0; i < 16; i++) blk[i] >>= 6;
+}
+
+// argmin with the reference's strict-< row-major scan: lowest cost, then lowest scan index
+__device__ __forceinline__ void better(double &c, int &i, double c2, int i2) {
+  if (c2 < c || (c2 == c && i2 < i)) {
+    c = c2;
+    i = i2;
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void block_argmin(double &c, int &i, double *sc, int *si) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
+    const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+    better(c, i, c2, i2);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    sc[warp] = c;
+    si[warp] = i;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < NT / 32; w++) better(c, i, sc[w], si[w]);
+    sc[0] = c;
+    si[0] = i;
+  }
+  __syncthreads();
+  c = sc[0];
+  i = si[0];
+}
+
+// ---------------------------------------------------------------- filters
+
+// lowPassFilter, filter.cpp:214-233
+__global__ void lowpass_kernel(const uint8_t *__restrict__ in, int w, int h, uint8_t *__restrict__ out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= w) return;
+  double sum = 0;
+  for (int m = y - 1; m <= y + 1; m++) {
+    if (m < 0 || m >= h) continue;
+    for (int n = x - 1; n <= x + 1; n++) {
+      if (n < 0 || n >= w) continue;
+      sum += (double)in[m * w + n];
+    }
+  }
+  out[y * w + x] = (uint8_t)(sum / 9);
+}
+
+// FIR_filter, filter.cpp:55-117, on the output window it keeps.  The taps are
+// the separable (1,-5,20,20,-5,1) half-pel filter: /32 horizontally or
+// vertically, /1024 at the centre position; zero taps of the reference's 6x6
+// tables are skipped (adding +0 to the running sum never changes it).
+__global__ void fir_kernel(const uint8_t *__restrict__ in, int w, int h, uint8_t *__restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+  const int w2 = w << 1;
+  if (j >= w2) return;
+  const double tap[6] = {1.0, -5.0, 20.0, 20.0, -5.0, 1.0};
+  const int sub = (j & 1) + ((i & 1) << 1);
+  const int cy = i / 2, cx = j / 2;
+  auto px = [&](int yy, int xx) {
+    yy = yy < 0 ? 0 : (yy > h - 1 ? h - 1 : yy);
+    xx = xx < 0 ? 0 : (xx > w - 1 ? w - 1 : xx);
+    return (double)in[yy * w + xx];
+  };
+  uint8_t v;
+  if (sub == 0) {
+    v = (uint8_t)px(cy, cx);
+  } else {
+    double sum = 0.0;
+    if (sub == 1) {
+      for (int jj = 0; jj < 6; jj++) sum += (tap[jj] / 32.0) * px(cy, cx - 2 + jj);
+    } else if (sub == 2) {
+      for (int ii = 0; ii < 6; ii++) sum += (tap[ii] / 32.0) * px(cy - 2 + ii, cx);
+    } else {
+      for (int ii = 0; ii < 6; ii++)
+        for (int jj = 0; jj < 6; jj++) sum += ((tap[ii] * tap[jj]) / 1024.0) * px(cy - 2 + ii, cx - 2 + jj);
+    }
+    int r = (int)(sum + 0.5);
+    v = (uint8_t)(r < 0 ? 0 : (r > 255 ? 255 : r));
+  }
+  out[i * w2 + j] = v;
+}
+
+cudaError_t launch_ref_planes(const uint8_t *recon, int w, int h, uint8_t *lp, uint8_t *ip, cudaStream_t s) {
+  lowpass_kernel<<<dim3((w + 127) / 128, h), 128, 0, s>>>(recon, w, h, lp);
+  fir_kernel<<<dim3((2 * w + 127) / 128, 2 * h), 128, 0, s>>>(recon, w, h, ip);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------- side-info creation
+
+// forwardME, sideInfoCreation.cpp:61-118: per 16x16 block of the future
+// low-pass frame, full search of +-32 pixels in the past low-pass frame.
+template <int NT>
+__global__ void __launch_bounds__(NT) forward_me_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, h = F.h, b16w = w / 16;
+  const int i = blockIdx.x;
+  const int top = (i / b16w) << 4, left = (i % b16w) << 4;
+  int st = top - SEARCH_R, sb = top + SEARCH_R, sl = left - SEARCH_R, sr = left + SEARCH_R;
+  if (st < 0) st = 0;
+  if (sb > h - 16) sb = h - 16;
+  if (sl < 0) sl = 0;
+  if (sr > w - 16) sr = w - 16;
+  const int ww = sr - sl + 16, wh = sb - st + 16;  // staged window (<= 80x80)
+  __shared__ uint8_t win[80 * 80];
+  __shared__ uint8_t blk[256];
+  __shared__ double sc[NT / 32];
+  __shared__ int sidx[NT / 32];
+  for (int k = threadIdx.x; k < ww * wh; k += NT) {
+    const int y = k / ww, x = k - y * ww;
+    win[k] = F.past_lp[(st + y) * w + sl + x];
+  }
+  for (int k = threadIdx.x; k < 256; k += NT) blk[k] = F.future_lp[(top + (k >> 4)) * w + left + (k & 15)];
+  __syncthreads();
+  const int cw = sr - sl + 1, nc = cw * (sb - st + 1);
+  double best = 1e300;
+  int bi = 0x7fffffff;
+  for (int c = threadIdx.x; c < nc; c += NT) {
+    const int py = c / cw, pxo = c - py * cw;
+    int sad = 0;
+    for (int m = 0; m < 16; m++) {
+      const uint8_t *wr = win + (py + m) * ww + pxo;
+      const uint8_t *br = blk + m * 16;
+#pragma unroll
+      for (int n = 0; n < 16; n++) sad += abs((int)br[n] - (int)wr[n]);
+    }
+    const double vx = (double)(sl + pxo - left), vy = (double)(st + py - top);
+    const double cost = cost_func((double)sad, vx, vy);
+    if (cost < 10000000.0) better(best, bi, cost, c);
+  }
+  block_argmin<NT>(best, bi, sc, sidx);
+  if (threadIdx.x == 0) {
+    MVd v{};
+    if (bi != 0x7fffffff) {
+      const int py = st + bi / cw, px = sl + bi % cw;
+      v.px = (double)px;
+      v.py = (double)py;
+      v.vx = (double)(px - left);
+      v.vy = (double)(py - top);
+    }
+    F.fmv[i] = v;
+    F.holes[2 * i] = (double)left * F.ipc + (double)v.px * F.ifc;
+    F.holes[2 * i + 1] = (double)top * F.ipc + (double)v.py * F.ifc;
+  }
+}
+
+// forwardME, sideInfoCreation.cpp:120-142 (nearest projected hole per
+// macroblock) and the half-pel scaling of createSideInfo (:511-521)
+__global__ void forward_me_post_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, h = F.h, b16w = w / 16, b16n = b16w * (h / 16);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= b16n) return;
+  const int top = (i / b16w) << 4, left = (i % b16w) << 4;
+  const double maxd = w * w + h * h;
+  double mind = maxd;
+  int bj = -1;
+  for (int j = 0; j < b16n; j++) {
+    const double hx = F.holes[2 * j], hy = F.holes[2 * j + 1];
+    const double d = (left - hx) * (left - hx) + (top - hy) * (top - hy);
+    if (d < mind) {
+      mind = d;
+      bj = j;
+    }
+  }
+  MVd b{};
+  if (bj >= 0) b = F.fmv[bj];
+  MVd o;
+  o.fx = (double)end_point(left, -b.vx, F.ifc, 0, w - 16);
+  o.fy = (double)end_point(top, -b.vy, F.ifc, 0, h - 16);
+  o.px = (double)end_point(left, b.vx, F.ipc, 0, w - 16);
+  o.py = (double)end_point(top, b.vy, F.ipc, 0, h - 16);
+  o.vx = o.px - o.fx;
+  o.vy = o.py - o.fy;
+  // half-pel units
+  o.fx *= 2;
+  o.fy *= 2;
+  o.px *= 2;
+  o.py *= 2;
+  o.vx = o.px - o.fx;
+  o.vy = o.py - o.fy;
+  F.mb_mv[i] = o;
+}
+
+// bidirectME, sideInfoCreation.cpp:235-310.  The reference visits blocks in
+// raster order and updates the vectors in place; a block's search window uses
+// its top and left neighbours' updated and its bottom and right neighbours'
+// previous vectors.  Blocks on one anti-diagonal are therefore independent:
+// this single-block-per-frame kernel walks the anti-diagonals, one warp per
+// block, which is equivalent to the raster order.
+template <int NT>
+__global__ void __launch_bounds__(NT) bidirect_me_kernel(FrameDev *frames, int bl) {
+  FrameDev &F = frames[blockIdx.x];
+  if (!F.active) return;
+  MVd *mv = bl == 16 ? F.mb_mv : F.blk_mv;
+  const int w = F.w, h = F.h, bh = h / bl, bw = w / bl, w2 = w << 1, bl2 = bl << 1;
+  const int srb = (h << 1) - bl2, srr = w2 - bl2;
+  const double scale = F.ipc / F.ifc;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint8_t *fut = F.future_ip, *pas = F.past_ip;
+  for (int d = 0; d < bh + bw - 1; d++) {
+    const int i0 = d - (bw - 1) > 0 ? d - (bw - 1) : 0;
+    const int i1 = d < bh - 1 ? d : bh - 1;
+    for (int i = i0 + warp; i <= i1; i += NT / 32) {
+      const int j = d - i;
+      const int bi = i * bw + j;
+      const int y2 = i * bl2, x2 = j * bl2;
+      const int st = (i - 1 >= 0) ? (int)mv[bi - bw].fy + bl2 : (int)mv[bi].fy;
+      const int sb = (i + 1 < bh) ? (int)mv[bi + bw].fy - bl2 : (int)mv[bi].fy;
+      const int sl = (j - 1 >= 0) ? (int)mv[bi - 1].fx + bl2 : (int)mv[bi].fx;
+      const int sr = (j + 1 < bw) ? (int)mv[bi + 1].fx - bl2 : (int)mv[bi].fx;
+      const int cw = sr - sl + 1, chh = sb - st + 1;
+      const int nc = (cw > 0 && chh > 0) ? cw * chh : 0;
+      double best = 1e300;
+      int bc = 0x7fffffff;
+      for (int c = lane; c < nc; c += 32) {
+        const int fy = st + c / cw, fx = sl + c % cw;
+        const int py = end_point(y2, (double)(y2 - fy), scale, 0, srb);
+        const int px = end_point(x2, (double)(x2 - fx), scale, 0, srr);
+        int mad = 0;
+        for (int m = 0; m < bl2; m += 2) {
+          const uint8_t *pr = pas + (py + m) * w2 + px;
+          const uint8_t *fr = fut + (fy + m) * w2 + fx;
+          for (int n = 0; n < bl2; n += 2) mad += abs((int)fr[n] - (int)pr[n]);
+        }
+        const double cost = cost_func((double)mad, (double)(px - fx), (double)(py - fy));
+        if (cost < 10000000.0) better(best, bc, cost, c);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double c2 = __shfl_xor_sync(0xffffffffu, best, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bc, o);
+        better(best, bc, c2, i2);
+      }
+      if (lane == 0 && bc != 0x7fffffff) {
+        const int fy = st + bc / cw, fx = sl + bc % cw;
+        const int py = end_point(y2, (double)(y2 - fy), scale, 0, srb);
+        const int px = end_point(x2, (double)(x2 - fx), scale, 0, srr);
+        MVd b;
+        b.fx = (double)fx;
+        b.fy = (double)fy;
+        b.px = (double)px;
+        b.py = (double)py;
+        b.vx = (double)(px - fx);
+        b.vy = (double)(py - fy);
+        mv[bi] = b;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// createSideInfo, sideInfoCreation.cpp:524-545: 8x8 vectors initialised
+// from their macroblock's vector
+__global__ void init_blk_mv_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, h = F.h, b8w = w / 8, b8n = b8w * (h / 8), b16w = w / 16;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b8n) return;
+  const int i = k / b8w, j = k % b8w;
+  const int srb = (h - 8) << 1, srr = (w - 8) << 1;
+  const int y2 = i << 4, x2 = j << 4;
+  const MVd v = F.mb_mv[(i >> 1) * b16w + (j >> 1)];
+  MVd o;
+  o.fx = (double)end_point(x2, -v.vx, F.ifc, 0, srr);
+  o.fy = (double)end_point(y2, -v.vy, F.ifc, 0, srb);
+  o.px = (double)end_point(x2, v.vx, F.ipc, 0, srr);
+  o.py = (double)end_point(y2, v.vy, F.ipc, 0, srb);
+  o.vx = o.px - o.fx;
+  o.vy = o.py - o.fy;
+  F.blk_mv[k] = o;
+}
+
+// motionFilterAndComp, sideInfoCreation.cpp:325-342: mean squared error per 8x8 block
+__global__ void mfc_mse_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, h = F.h, b8n = (w / 8) * (h / 8), w2 = w << 1;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b8n) return;
+  const MVd v = F.blk_mv[k];
+  const int fy = (int)v.fy, fx = (int)v.fx, py = (int)v.py, px = (int)v.px;
+  double s = 0.0;
+  for (int m = 0; m < 16; m += 2)
+    for (int n = 0; n < 16; n += 2) {
+      const double d = (double)F.future_ip[(fy + m) * w2 + fx + n] - (double)F.past_ip[(py + m) * w2 + px + n];
+      s += d * d;
+    }
+  F.mse[k] = s / 64;
+}
+
+// motionFilterAndComp, sideInfoCreation.cpp:344-405: weighted vector median
+// over the 3x3 neighbourhood, then the new end points
+__global__ void mfc_wvmf_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, h = F.h, b8w = w / 8, b8h = h / 8, b8n = b8w * b8h;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b8n) return;
+  const int i = k / b8w, j = k % b8w;
+  const int srb = (h << 1) - 16, srr = (w << 1) - 16;
+  const int y2 = i << 4, x2 = j << 4;
+  int nbr[9], cnt = 0;
+  for (int m = i - 1; m <= i + 1; m++) {
+    if (m < 0 || m >= b8h) continue;
+    for (int n = j - 1; n <= j + 1; n++) {
+      if (n < 0 || n >= b8w) continue;
+      nbr[cnt++] = m * b8w + n;
+    }
+  }
+  const MVd *mv = F.blk_mv;
+  const double *mse = F.mse;
+  double minw = 0.0;
+  int bestb = nbr[0];
+  for (int q = 1; q < cnt; q++) {
+    const int o = nbr[q];
+    const double dx = mv[bestb].vx - mv[o].vx, dy = mv[bestb].vy - mv[o].vy;
+    minw += mse[bestb] / mse[o] * sqrt(dx * dx + dy * dy);
+  }
+  for (int c = 1; c < cnt; c++) {
+    const int cb = nbr[c];
+    double wv = 0.0;
+    for (int q = 0; q < cnt; q++) {
+      if (c == q) continue;
+      const int o = nbr[q];
+      const double dx = mv[cb].vx - mv[o].vx, dy = mv[cb].vy - mv[o].vy;
+      wv += mse[cb] / mse[o] * sqrt(dx * dx + dy * dy);
+    }
+    if (wv < minw) {
+      minw = wv;
+      bestb = cb;
+    }
+  }
+  const double vx = mv[bestb].vx, vy = mv[bestb].vy;
+  MVd o;
+  o.fx = (double)end_point(x2, -vx, F.ifc, 0, srr);
+  o.fy = (double)end_point(y2, -vy, F.ifc, 0, srb);
+  o.px = (double)end_point(x2, vx, F.ipc, 0, srr);
+  o.py = (double)end_point(y2, vy, F.ipc, 0, srb);
+  o.vx = o.px - o.fx;
+  o.vy = o.py - o.fy;
+  F.blk_mv2[k] = o;
+}
+
+// motionFilterAndComp, sideInfoCreation.cpp:407-434 (bidirectional motion
+// compensation -> side information and residue), then copyIntraBlkToSideInfo
+// (intra.cpp:271-288)
+__global__ void mfc_comp_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, h = F.h, w2 = w << 1;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.z;
+  if (x >= w || y >= h) return;
+  const int b8 = (y >> 3) * (w >> 3) + (x >> 3);
+  const MVd v = F.blk_mv2[b8];
+  const int m = (y & 7) << 1, n = (x & 7) << 1;
+  const int fi = ((int)v.fy + m) * w2 + (int)v.fx + n, pi = ((int)v.py + m) * w2 + (int)v.px + n;
+  const uint8_t fv = F.future_ip[fi], pv = F.past_ip[pi];
+  uint8_t s = (uint8_t)(int)((double)fv * F.ifc + (double)pv * F.ipc);
+  if (F.mode[b8] == DVC_INTRA_B) s = F.recon[y * w + x];
+  F.si[y * w + x] = s;
+  F.residue[y * w + x] = ((int)fv - (int)pv) >> 1;
+}
+
+// copySkipBlkToRecons, skipBlock.cpp:3-22: skip blocks take the past frame's pixels
+__global__ void skip_copy_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || F.skip_mode != 1) return;
+  const int w = F.w;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.z;
+  if (x >= w) return;
+  if (F.mode[(y >> 3) * (w >> 3) + (x >> 3)] == DVC_SKIP_B) F.recon[y * w + x] = F.past[y * w + x];
+}
+
+// ------------------------------------------- transforms and noise parameters
+
+// forwardTransform (transform.cpp:153-190) of the residue, every 4x4 block
+__global__ void residue_transform_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, b4w = w / 4, b4n = b4w * (F.h / 4);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b4n) return;
+  const int i = k / b4w, j = k % b4w;
+  int b[16];
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) b[4 * m + n] = F.residue[(4 * i + m) * w + 4 * j + n];
+  forward44(b);
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) F.side_trans[(4 * i + m) * w + 4 * j + n] = b[4 * m + n];
+}
+
+// noiseParameter, noiseModel.cpp:14-45: band mean and variance of |T| over
+// every 4x4 block.  The variance accumulates squares past 2^24, so each band's
+// sums run sequentially in raster block order, one thread per band.
+__global__ void noise_band_stats_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.x];
+  if (!F.active) return;
+  const int band = threadIdx.x;
+  if (band >= 16) return;
+  const int index = c_zigzag[band];
+  // bands are coded while Qbits > 0 in zig-zag order; later ones are unused
+  bool coded = true;
+  for (int b = 0; b <= band; b++) coded = coded && F.qbits[c_zigzag[b]] > 0;
+  if (!coded) return;
+  const int w = F.w, b4w = w / 4, b4h = F.h / 4, b4n = b4w * b4h;
+  float mean = 0.0f, var = 0.0f;
+  for (int i = 0; i < b4h; i++)
+    for (int j = 0; j < b4w; j++) {
+      const float c = fabsf((float)F.side_trans[(4 * i + (index >> 2)) * w + 4 * j + (index & 3)]);
+      mean += c;
+      var += c * c;
+    }
+  mean /= (float)b4n;
+  var = var / (float)b4n - mean * mean;
+  F.band_mean[band] = mean;
+  F.band_var[band] = var;
+}
+
+// noiseParameter, noiseModel.cpp:47-73: alpha per WZ coefficient of coded bands
+__global__ void noise_alpha_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, b4w = w / 4, b4n = b4w * (F.h / 4);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b4n) return;
+  const int i = k / b4w, j = k % b4w;
+  if (F.mode[(i >> 1) * (w >> 3) + (j >> 1)] != DVC_WZ_B) return;
+  int band = 0, index = c_zigzag[0];
+  while (band < 16 && F.qbits[index] > 0) {
+    const int ci = (4 * i + (index >> 2)) * w + 4 * j + (index & 3);
+    const float t = fabsf((float)F.side_trans[ci]);  // the reference stores |T| back first
+    const float d = (float)(int)t - F.band_mean[band];
+    const float d2 = d * d;
+    F.alpha[ci] = d2 > F.band_var[band] ? sqrtf(2 / d2) : sqrtf(2 / F.band_var[band]);
+    band++;
+    if (band < 16) index = c_zigzag[band];
+  }
+}
+
+// overCompleteTransform, transform.cpp:275-298: the 4x4 transform of the side
+// information at every pixel offset (values fit 16 bits)
+__global__ void over_complete_kernel(FrameDev *frames, int band) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !in_step(F, band, 0)) return;
+  const int w = F.w, srw = w - 3;
+  const int left = blockIdx.x * blockDim.x + threadIdx.x, top = blockIdx.z;
+  if (left >= srw) return;
+  int b[16];
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) b[4 * m + n] = F.si[(top + m) * w + left + n];
+  forward44(b);
+  int16_t *o = F.oct + ((size_t)top * srw + left) * 16;
+#pragma unroll
+  for (int c = 0; c < 16; c += 2) {
+    const uint32_t pk = (uint32_t)(uint16_t)(int16_t)b[c] | ((uint32_t)(uint16_t)(int16_t)b[c + 1] << 16);
+    reinterpret_cast<uint32_t *>(o)[c >> 1] = pk;
+  }
+}
+
+// init_si_ML, motionLearning.cpp:49-68 (every block), and initSMF (:6-47) for WZ blocks
+__global__ void init_ml_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active) return;
+  const int w = F.w, h = F.h, b4w = w / 4, b4n = b4w * (h / 4), srw = w - 3;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b4n) return;
+  const int i = k / b4w, j = k % b4w;
+  const int16_t *t = F.oct + ((size_t)(4 * i) * srw + 4 * j) * 16;
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) F.side_trans[(4 * i + m) * w + 4 * j + n] = t[4 * m + n];
+  const int s = F.sir_of_blk[k];
+  if (s < 0) return;
+  const int top = 4 * i, left = 4 * j;
+  int st = top - LEARN_R, sb = top + LEARN_R, sl = left - LEARN_R, sr = left + LEARN_R;
+  if (st < 0) st = 0;
+  if (sb > h - 4) sb = h - 4;
+  if (sl < 0) sl = 0;
+  if (sr > w - 4) sr = w - 4;
+  float *p = F.smf + (size_t)s * ML_N;
+  int q = 0;
+  for (int m = st; m <= sb; m++)
+    for (int n = sl; n <= sr; n++) p[q++] = (m == top && n == left) ? 1.0f : 0.0f;
+}
+
+// SMF window of a WZ block (initSMF bounds, motionLearning.cpp:16-27)
+struct Win {
+  int st, sb, sl, sr;
+};
+__device__ __forceinline__ Win ml_window(int top, int left, int w, int h) {
+  Win r{top - LEARN_R, top + LEARN_R, left - LEARN_R, left + LEARN_R};
+  if (r.st < 0) r.st = 0;
+  if (r.sb > h - 4) r.sb = h - 4;
+  if (r.sl < 0) r.sl = 0;
+  if (r.sr > w - 4) r.sr = w - 4;
+  return r;
+}
+
+// ------------------------------------------------------ correlation noise
+
+// noiseDistribution, noiseModel.cpp:77-132: per WZ block, the (mixture of)
+// Laplacian pdf over every coefficient value of the band.  The exponential
+// depends only on the integer distance d = |k - range - s_m|, so each block
+// first tabulates expf(-alpha*d) (the same float expression) for every d it
+// needs, then sums the 81-candidate mixture in the reference's order.
+#define NOISE_TAB 4096
+template <int NT>
+__global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev xt, int band) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !in_step(F, band, 0)) return;
+  const int s_idx = blockIdx.x;
+  if (s_idx >= F.nsir) return;
+  const int w = F.w, h = F.h, b4w = w / 4, srw = w - 3;
+  const int index = c_zigzag[band];
+  const int range = F.crange[index];
+  const int blk = F.sir[s_idx];
+  const int top = (blk / b4w) << 2, left = (blk % b4w) << 2;
+  __shared__ float etab[NOISE_TAB];
+  __shared__ float prob[ML_N];
+  __shared__ int sc[ML_N];
+  __shared__ int s_n, s_dmax;
+  float *out = F.pdf + (size_t)s_idx * F.pdf_stride;
+  if (index == 0) {
+    const float a = F.alpha[top * w + left];
+    const int s = F.oct[((size_t)top * srw + left) * 16];
+    for (int k = threadIdx.x; k < range; k += NT) out[k] = xl_expf(xt, -a * (float)abs(k - s));
+    return;
+  }
+  const float a = F.alpha[(top + (index >> 2)) * w + left + (index & 3)];
+  if (threadIdx.x == 0) {
+    const Win wn = ml_window(top, left, w, h);
+    int q = 0, mx = 0;
+    for (int m = wn.st; m <= wn.sb; m++)
+      for (int n = wn.sl; n <= wn.sr; n++) {
+        const int v = F.oct[((size_t)m * srw + n) * 16 + index];
+        sc[q] = v;
+        prob[q] = F.smf[(size_t)s_idx * ML_N + q];
+        mx = max(mx, abs(v));
+        q++;
+      }
+    s_n = q;
+    s_dmax = range + mx;
+  }
+  __syncthreads();
+  const int nm = s_n, dmax = s_dmax;
+  const int tab = dmax < NOISE_TAB ? dmax + 1 : NOISE_TAB;
+  for (int d = threadIdx.x; d < tab; d += NT) etab[d] = xl_expf(xt, -a * (float)d);
+  __syncthreads();
+  const int rmax = 2 * range + 1;
+  for (int k = threadIdx.x; k < rmax; k += NT) {
+    const int pc = k - range;
+    float sum = 0.0f;
+    for (int m = 0; m < nm; m++) {
+      const int d = abs(pc - sc[m]);
+      const float e = d < NOISE_TAB ? etab[d] : xl_expf(xt, -a * (float)d);
+      sum += prob[m] * e;
+    }
+    out[k] = sum;
+  }
+}
+
+// condBitProb, noiseModel.cpp:191-310: LR = p0/p1 from sequential interval
+// sums of the pdf, one thread per 4x4 block.  Non-WZ blocks get the
+// reference's certain-zero ratio when the frame has skip or intra blocks.
+__global__ void cond_bit_kernel(FrameDev *frames, int band, int bit) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !in_step(F, band, bit)) return;
+  const int w = F.w, b4w = w / 4, b4n = b4w * (F.h / 4);
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= b4n) return;
+  const int s_idx = F.sir_of_blk[k];
+  if (s_idx < 0) {
+    if (F.skip_mode == 1 || F.intra_mode == 1) F.lr[k] = 0.9999f / 0.0001f;
+    return;
+  }
+  const int index = c_zigzag[band], step = F.step[index], range = F.crange[index];
+  const int i = k / b4w, j = k % b4w;
+  const int rc = F.recons_trans[(4 * i + (index >> 2)) * w + 4 * j + (index & 3)];
+  const float *p = F.pdf + (size_t)s_idx * F.pdf_stride;
+  const int iq = (1 << (bit - 1)) - 1;
+  float p0 = 0.0f, p1 = 0.0f;
+  // interval ends are clamped to the pdf row; consistent bitstreams never reach the clamp
+  if (index == 0) {
+    const int b0l = rc << bit, b1l = ((rc << 1) + 1) << (bit - 1);
+    const int b0u = b0l + iq, b1u = b1l + iq;
+    const int v0l = b0l * step, v1l = b1l * step, v0u = (b0u + 1) * step, v1u = (b1u + 1) * step;
+    for (int q = max(v0l, 0); q < min(v0u, range); q++) p0 += p[q];
+    for (int q = max(v1l, 0); q < min(v1u, range); q++) p1 += p[q];
+  } else {
+    const int ls = F.level_shift[index];
+    const int b0l = (rc << bit) - ls;
+    const int b1l = (((rc << 1) + 1) << (bit - 1)) - ls;
+    const int b0u = b0l + iq;
+    int b1u = b1l + iq;
+    if (b1u > ls) b1u = ls;
+    const int v0l = (b0l <= 0) ? (b0l - 1) * step + 1 : b0l * step;
+    const int v1l = (b1l <= 0) ? (b1l - 1) * step + 1 : b1l * step;
+    const int v0u = ((b0u < 0) ? b0u * step + 1 : (b0u + 1) * step) + range;
+    const int v1u = ((b1u < 0) ? b1u * step + 1 : (b1u + 1) * step) + range;
+    const int len = 2 * range + 1;
+    for (int q = max(v0l + range, 0); q < min(v0u, len); q++) p0 += p[q];
+    for (int q = max(v1l + range, 0); q < min(v1u, len); q++) p1 += p[q];
+  }
+  p0 = p0 / (p0 + p1);
+  p1 = 1 - p0;
+  float lr;
+  if (p0 <= 0.0001)
+    lr = (float)(0.0001 / 0.9999);
+  else if (p0 >= 0.9999)
+    lr = (float)(0.9999 / 0.0001);
+  else
+    lr = p0 / p1;
+  F.lr[k] = lr;
+}
+
+// ------------------------------------------------------- reconstruction
+
+// reconstruction (reconstruction.cpp:184-289) of the band's coefficient, then
+// inverseTransform (transform.cpp:234-273) of the block; one thread per WZ block
+__global__ void recon_kernel(FrameDev *frames, int band) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !in_step(F, band, 0)) return;
+  const int s_idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s_idx >= F.nsir) return;
+  const int w = F.w, b4w = w / 4;
+  const int blk = F.sir[s_idx];
+  const int top = (blk / b4w) << 2, left = (blk % b4w) << 2;
+  if (band >= 0) {
+    const int index = c_zigzag[band], step = F.step[index];
+    const int ci = (top + (index >> 2)) * w + left + (index & 3);
+    int lo, hi;
+    if (index == 0) {
+      const int q = F.recons_trans[ci];
+      lo = q * step;
+      hi = (q + 1) * step;
+    } else {
+      const int q = F.recons_trans[ci] - F.level_shift[index];
+      if (q == 0) {
+        lo = -step + 1;
+        hi = step;
+      } else if (q > 0) {
+        lo = q * step;
+        hi = (q + 1) * step;
+      } else {
+        lo = (q - 1) * step + 1;
+        hi = q * step + 1;
+      }
+    }
+    const int sc = F.side_trans[ci];
+    const double a = F.alpha[ci];
+    int v;
+    if (a <= 0.0001) {
+      v = (lo + hi) / 2;
+    } else if (sc < lo) {
+      v = lo + dround(1.0 / a + (double)step / (1.0 - exp(a * (double)step)));
+    } else if (sc >= hi) {
+      v = hi - dround(1.0 / a + (double)step / (1.0 - exp(a * (double)step)));
+    } else {
+      const double r = sc - lo, d = hi - sc;
+      const double er = exp(-a * r), ed = exp(-a * d);
+      v = sc + dround(((r + 1.0 / a) * er - (d + 1.0 / a) * ed) / (2.0 - (er + ed)));
+    }
+    F.side_trans[ci] = v;
+    F.dbf[ci] = ((v ^ sc) != 0) ? 1 : 0;
+  }
+  int b[16];
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) b[4 * m + n] = F.side_trans[(top + m) * w + left + n];
+  inverse44(b);
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) {
+      const int c = b[4 * m + n];
+      F.recon[(top + m) * w + left + n] = (uint8_t)(c < 0 ? 0 : (c > 255 ? 255 : c));
+    }
+}
+
+// -------------------------------------------------- side-info refinement
+
+// updateSI + subPelRefine, sideInfoCreation.cpp:598-736: per WZ block, +-32
+// integer search against the past and future reconstructions (cost = SAD with
+// the motion-vector weight; strict-< row-major argmin), a +-1 half-pel
+// refinement in the interpolated frames, and the bidirectional average.
+template <int NT>
+__global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int band) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !in_step(F, band, 0)) return;
+  const int s_idx = blockIdx.x;
+  if (s_idx >= F.nsir) return;
+  const int w = F.w, h = F.h, b4w = w / 4, w2 = w << 1, h2 = h << 1;
+  const int blk = F.sir[s_idx];
+  const int top = (blk / b4w) << 2, left = (blk % b4w) << 2;
+  int st = top - SEARCH_R, sb = top + SEARCH_R, sl = left - SEARCH_R, sr = left + SEARCH_R;
+  if (st < 0) st = 0;
+  if (sb > h - 4) sb = h - 4;
+  if (sl < 0) sl = 0;
+  if (sr > w - 4) sr = w - 4;
+  const int ww = sr - sl + 4, wh = sb - st + 4;  // <= 68 x 68
+  __shared__ uint8_t wp[68 * 68], wf[68 * 68];
+  __shared__ int cur[16];
+  __shared__ double scp[NT / 32], scf[NT / 32];
+  __shared__ int sip[NT / 32], sif[NT / 32];
+  for (int k = threadIdx.x; k < ww * wh; k += NT) {
+    const int y = k / ww, x = k - y * ww;
+    wp[k] = F.past[(st + y) * w + sl + x];
+    wf[k] = F.future[(st + y) * w + sl + x];
+  }
+  if (threadIdx.x < 16) cur[threadIdx.x] = F.recon[(top + (threadIdx.x >> 2)) * w + left + (threadIdx.x & 3)];
+  __syncthreads();
+  const int cw = sr - sl + 1, nc = cw * (sb - st + 1);
+  double bp = 1e300, bf = 1e300;
+  int ip = 0x7fffffff, jf = 0x7fffffff;
+  for (int c = threadIdx.x; c < nc; c += NT) {
+    const int yo = c / cw, xo = c - yo * cw;
+    int sp = 0, sf = 0;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      const int base = (yo + m) * ww + xo;
+#pragma unroll
+      for (int n = 0; n < 4; n++) {
+        const int b = cur[4 * m + n];
+        sp += abs(b - (int)wp[base + n]);
+        sf += abs(b - (int)wf[base + n]);
+      }
+    }
+    const double vx = (double)((sl + xo - left) << 1), vy = (double)((st + yo - top) << 1);
+    const double wgt = 1.0 + (double)0.05f * sqrt(vx * vx + vy * vy);
+    const double cp = (double)sp * wgt, cf = (double)sf * wgt;
+    if (cp < 10000000.0) better(bp, ip, cp, c);
+    if (cf < 10000000.0) better(bf, jf, cf, c);
+  }
+  block_argmin<NT>(bp, ip, scp, sip);
+  block_argmin<NT>(bf, jf, scf, sif);
+  if (threadIdx.x == 0) {
+    int pbx = sl + ip % cw, pby = st + ip / cw, fbx = sl + jf % cw, fby = st + jf / cw;
+    // subPelRefine in the half-pel planes, no vector weight (sideInfoCreation.cpp:598-640)
+    for (int which = 0; which < 2; which++) {
+      const uint8_t *ref = which == 0 ? F.past_ip : F.future_ip;
+      int &bx = which == 0 ? pbx : fbx;
+      int &by = which == 0 ? pby : fby;
+      const int ix = bx << 1, iy = by << 1;
+      double minc = 10000000.0;
+      int nbx = bx, nby = by;
+      for (int di = -1; di <= 1; di++) {
+        const int tt = iy + di;
+        if (tt < 0 || tt > h2 - 8) continue;
+        for (int dj = -1; dj <= 1; dj++) {
+          const int ll = ix + dj;
+          if (ll < 0 || ll > w2 - 8) continue;
+          int sad = 0;
+          for (int m = 0; m < 4; m++)
+            for (int n = 0; n < 4; n++) sad += abs(cur[4 * m + n] - (int)ref[(tt + 2 * m) * w2 + ll + 2 * n]);
+          const double c = (double)sad;
+          if (c < minc) {
+            minc = c;
+            nbx = ll;
+            nby = tt;
+          }
+        }
+      }
+      bx = nbx;
+      by = nby;
+    }
+    for (int m = 0; m < 4; m++)
+      for (int n = 0; n < 4; n++) {
+        const double pv = (double)F.past_ip[(pby + 2 * m) * w2 + pbx + 2 * n];
+        const double fv = (double)F.future_ip[(fby + 2 * m) * w2 + fbx + 2 * n];
+        F.si[(top + m) * w + left + n] = (uint8_t)(int)(pv * F.ipc + fv * F.ifc);
+      }
+  }
+}
+
+// ------------------------------------------------------ motion learning
+
+// updateSMF, motionLearning.cpp:70-127: one warp per WZ block
+__global__ void update_smf_kernel(FrameDev *frames, XlmDev xt, int band) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !in_step(F, band, 0)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= F.nsir) return;
+  const int w = F.w, h = F.h, b4w = w / 4;
+  const int blk = F.sir[warp];
+  const int top = (blk / b4w) << 2, left = (blk % b4w) << 2;
+  const Win wn = ml_window(top, left, w, h);
+  const int cw = wn.sr - wn.sl + 1, nc = cw * (wn.sb - wn.st + 1);
+  float *p = F.smf + (size_t)warp * ML_N;
+  float pr[3];
+  for (int r = 0; r < 3; r++) {
+    const int q = lane + 32 * r;
+    pr[r] = 0.0f;
+    if (q < nc) {
+      const int m = wn.st + q / cw, n = wn.sl + q % cw;
+      float sse = 0.0f;
+      for (int ii = 0; ii < 4; ii++)
+        for (int jj = 0; jj < 4; jj++) {
+          const float d = (float)F.recon[(top + ii) * w + left + jj] - (float)F.si[(m + ii) * w + n + jj];
+          sse += d * d;
+        }
+      pr[r] = xl_expf(xt, (float)-0.01f * sse);
+    }
+  }
+  // sequential sum in candidate order
+  float sum = 0.0f;
+  for (int q = 0; q < nc; q++) {
+    const float v = __shfl_sync(0xffffffffu, pr[q >> 5], q & 31);
+    sum += v;
+  }
+  int center = 0;
+  {
+    const int cm = top - wn.st, cn = left - wn.sl;
+    center = cm * cw + cn;
+  }
+  for (int r = 0; r < 3; r++) {
+    const int q = lane + 32 * r;
+    if (q < nc) p[q] = sum > 0.0 ? pr[r] / sum : (q == center ? 1.0f : pr[r]);
+  }
+}
+
+// update_si_ML, motionLearning.cpp:129-160: ML side coefficients of bands >= first_band
+__global__ void update_ml_kernel(FrameDev *frames, int band) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !in_step(F, band, 0)) return;
+  const int first_band = band + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s_idx = t >> 4, c = t & 15;
+  if (s_idx >= F.nsir || c < first_band) return;
+  const int w = F.w, h = F.h, b4w = w / 4, srw = w - 3;
+  const int index = c_zigzag[c];
+  const int blk = F.sir[s_idx];
+  const int top = (blk / b4w) << 2, left = (blk % b4w) << 2;
+  const Win wn = ml_window(top, left, w, h);
+  const float *p = F.smf + (size_t)s_idx * ML_N;
+  float acc = 0.0f;
+  int q = 0;
+  for (int m = wn.st; m <= wn.sb; m++)
+    for (int n = wn.sl; n <= wn.sr; n++) {
+      acc += p[q] * (float)(F.oct[((size_t)m * srw + n) * 16 + index]);
+      q++;
+    }
+  F.side_trans[(top + (index >> 2)) * w + left + (index & 3)] = (int)acc;
+}
+
+// ------------------------------------------------------------- launchers
+
+static inline dim3 g2(int n, int tpb, int frames) { return dim3((n + tpb - 1) / tpb, frames); }
+
+cudaError_t launch_side_info(FrameDev *fr, int nf, int w, int h, cudaStream_t s) {
+  const int b16n = (w / 16) * (h / 16), b8n = (w / 8) * (h / 8);
+  forward_me_kernel<256><<<dim3(b16n, nf), 256, 0, s>>>(fr);
+  forward_me_post_kernel<<<g2(b16n, 128, nf), 128, 0, s>>>(fr);
+  bidirect_me_kernel<1024><<<nf, 1024, 0, s>>>(fr, 16);
+  init_blk_mv_kernel<<<g2(b8n, 128, nf), 128, 0, s>>>(fr);
+  bidirect_me_kernel<1024><<<nf, 1024, 0, s>>>(fr, 8);
+  mfc_mse_kernel<<<g2(b8n, 128, nf), 128, 0, s>>>(fr);
+  mfc_wvmf_kernel<<<g2(b8n, 128, nf), 128, 0, s>>>(fr);
+  mfc_comp_kernel<<<dim3((w + 127) / 128, nf, h), 128, 0, s>>>(fr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_frame_prep(FrameDev *fr, int nf, int w, int h, cudaStream_t s) {
+  const int b4n = (w / 4) * (h / 4);
+  residue_transform_kernel<<<g2(b4n, 128, nf), 128, 0, s>>>(fr);
+  noise_band_stats_kernel<<<nf, 32, 0, s>>>(fr);
+  noise_alpha_kernel<<<g2(b4n, 128, nf), 128, 0, s>>>(fr);
+  over_complete_kernel<<<dim3((w - 3 + 127) / 128, nf, h - 3), 128, 0, s>>>(fr, -1);
+  init_ml_kernel<<<g2(b4n, 128, nf), 128, 0, s>>>(fr);
+  skip_copy_kernel<<<dim3((w + 127) / 128, nf, h), 128, 0, s>>>(fr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_noise_dist(FrameDev *fr, int nf, int max_nsir, const XlmDev &xt, int band, cudaStream_t s) {
+  noise_dist_kernel<256><<<dim3(max_nsir, nf), 256, 0, s>>>(fr, xt, band);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cond_bit(FrameDev *fr, int nf, int w, int h, int band, int bit, cudaStream_t s) {
+  cond_bit_kernel<<<g2((w / 4) * (h / 4), 128, nf), 128, 0, s>>>(fr, band, bit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_band_end(FrameDev *fr, int nf, int w, int h, int max_nsir, int band, const XlmDev &xt,
+                            cudaStream_t s) {
+  recon_kernel<<<g2(max_nsir, 128, nf), 128, 0, s>>>(fr, band);
+  update_si_kernel<128><<<dim3(max_nsir, nf), 128, 0, s>>>(fr, band);
+  over_complete_kernel<<<dim3((w - 3 + 127) / 128, nf, h - 3), 128, 0, s>>>(fr, band);
+  update_smf_kernel<<<g2(max_nsir * 32, 128, nf), 128, 0, s>>>(fr, xt, band);
+  update_ml_kernel<<<g2(max_nsir * 16, 128, nf), 128, 0, s>>>(fr, band);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_final_inverse(FrameDev *fr, int nf, int max_nsir, cudaStream_t s) {
+  recon_kernel<<<g2(max_nsir, 128, nf), 128, 0, s>>>(fr, -1);
+  return cudaGetLastError();
+}
+
+}  // namespace dvc

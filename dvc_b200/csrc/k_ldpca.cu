@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(NT, 1)
     ldpca_ladder_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, XlmDev xt, int max_iter) {
   extern __shared__ __align__(16) uint8_t smem[];
   const LdpcaJob J = jobs[blockIdx.x];
+  if (!J.active) return;
   const int n = L.n, E = L.e, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   float *msg = reinterpret_cast<float *>(smem);
   float *llr = msg + E;

@@ -61,7 +61,21 @@ def _declare_frame_api(L):
             f.restype = C.c_int
 
 
-FRAME_API = {}
+class WZFrame(C.Structure):
+    """dvc_wz_frame (include/dvc_b200.h)."""
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("qindex", C.c_int),
+                ("past_idx", C.c_int), ("future_idx", C.c_int), ("cur_idx", C.c_int),
+                ("past", C.c_void_p), ("future", C.c_void_p), ("mode", C.c_void_p),
+                ("skip_mode", C.c_int), ("intra_mode", C.c_int), ("ac_range", C.c_void_p),
+                ("crc", C.c_void_p), ("acc_synd", C.c_void_p), ("recon", C.c_void_p),
+                ("wz_bits", C.c_int), ("plane_results", C.c_void_p), ("plane_entropy", C.c_void_p),
+                ("deblock_flag", C.c_void_p)]
+
+
+FRAME_API = {
+    "dvc_decode_wz_frames": [C.c_void_p, C.c_int, C.POINTER(WZFrame)],
+    "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
+}
 
 
 def _ptr(a):
@@ -127,3 +141,50 @@ class Context:
         self.check(lib().dvc_LdpcaDecoder(self._h, len(lr), _ptr(lr), _ptr(acc), _ptr(dec), C.byref(rate),
                                           C.c_ubyte(int(crc)), C.c_float(rate_lower_bound)))
         return dec, rate.value, lr
+
+    def debug_wz_frame(self, item):
+        """One frame through dvc_debug_wz_frame: the decode result plus si_initial, alpha, si_final."""
+        return self.decode_wz_frames([item], debug=True)[0]
+
+    def decode_wz_frames(self, items, debug=False):
+        """Decode independent WZ frames as one batch.
+
+        items: list of dicts with keys width, height, qindex, past_idx, future_idx,
+        cur_idx, past, future (uint8 HxW), mode (uint8 or None), skip_mode, intra_mode,
+        ac_range (16 ints), crc (uint8 [qbits]), acc (uint8 [qbits, n/8]), recon
+        (uint8 HxW with intra pixels, or None).  Returns a list of dicts with
+        recon, wz_bits, planes ([qbits,4] int32), entropy, deblock_flag.
+        """
+        keep = []
+        arr = (WZFrame * len(items))()
+        outs = []
+        for i, it in enumerate(items):
+            w, h = it["width"], it["height"]
+            past = np.ascontiguousarray(it["past"], np.uint8)
+            fut = np.ascontiguousarray(it["future"], np.uint8)
+            mode = None if it.get("mode") is None else np.ascontiguousarray(it["mode"], np.uint8)
+            acr = np.ascontiguousarray(it["ac_range"], np.int32)
+            crc = np.ascontiguousarray(it["crc"], np.uint8)
+            acc = np.ascontiguousarray(it["acc"], np.uint8)
+            rec = np.zeros((h, w), np.uint8) if it.get("recon") is None else np.ascontiguousarray(it["recon"], np.uint8).copy()
+            qb = len(crc)
+            planes = np.zeros((qb, 4), np.int32)
+            ent = np.zeros(qb, np.float32)
+            dbf = np.zeros((h, w), np.uint8)
+            keep += [past, fut, mode, acr, crc, acc]
+            arr[i] = WZFrame(w, h, it["qindex"], it["past_idx"], it["future_idx"], it["cur_idx"], _ptr(past),
+                             _ptr(fut), _ptr(mode), it.get("skip_mode", 0), it.get("intra_mode", 0), _ptr(acr),
+                             _ptr(crc), _ptr(acc), _ptr(rec), 0, _ptr(planes), _ptr(ent), _ptr(dbf))
+            outs.append(dict(recon=rec, planes=planes, entropy=ent, deblock_flag=dbf))
+        if debug:
+            w, h = items[0]["width"], items[0]["height"]
+            si0 = np.zeros((h, w), np.uint8)
+            si1 = np.zeros((h, w), np.uint8)
+            alpha = np.zeros((h, w), np.float32)
+            self.check(lib().dvc_debug_wz_frame(self._h, arr, _ptr(si0), _ptr(alpha), _ptr(si1)))
+            outs[0].update(si_initial=si0, si_final=si1, alpha=alpha)
+        else:
+            self.check(lib().dvc_decode_wz_frames(self._h, len(items), arr))
+        for i, o in enumerate(outs):
+            o["wz_bits"] = arr[i].wz_bits
+        return outs

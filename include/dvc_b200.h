@@ -67,6 +67,46 @@ int dvc_ldpca_decode(dvc_ctx *ctx, int n, int count, const float *lr, const uint
 int dvc_LdpcaDecoder(dvc_ctx *ctx, int n, float *LR_intrinsic, const unsigned char *accumulatedSyndrome,
                      unsigned char *decoded, int *rate, unsigned char crc_encoder, float RateLowerBound);
 
+/* One Wyner-Ziv frame for dvc_decode_wz_frames (all buffers are host memory).
+ * The fields are what the reference's decodeGOP reads for one frame
+ * (DVC_Decoder.cpp:26-435): the two reconstructed reference frames, the parsed
+ * WZ-bitstream data of the frame (wzbitstream.cpp:13-126) and, for intra
+ * blocks, the pixels intraRecon produced. */
+typedef struct {
+  int width, height;           /* 176x144 or 352x288 */
+  int qindex;                  /* 1..8 */
+  int past_idx, future_idx, cur_idx; /* frame numbers (set the interpolation weights) */
+  const uint8_t *past;         /* [w*h] reconstructed past reference (luma) */
+  const uint8_t *future;       /* [w*h] reconstructed future reference */
+  const uint8_t *mode;         /* [w*h/64] 8x8 block modes 0 WZ, 1 intra, 2 skip; NULL = all WZ */
+  int skip_mode, intra_mode;   /* frame-level flags from the bitstream */
+  const int *ac_range;         /* [16] AC dynamic range per coefficient index */
+  const uint8_t *crc;          /* [qbits] CRC-8 per bitplane */
+  const uint8_t *acc_synd;     /* [qbits * w*h/128] accumulated syndromes, bitstream byte layout */
+  uint8_t *recon;              /* [w*h] in: intra-block pixels (if any); out: decoded frame before deblocking */
+  int wz_bits;                 /* out: 10 per coded AC band + sum over bitplanes of (m+8) */
+  int *plane_results;          /* out [qbits*4] or NULL: rate, first code, accepted code, BP iterations */
+  float *plane_entropy;        /* out [qbits] or NULL */
+  uint8_t *deblock_flag;       /* out [w*h] or NULL: coefficients changed by reconstruction */
+} dvc_wz_frame;
+
+/* Decode `count` WZ frames of one size as one batch on the device (frames
+ * must not depend on each other).  Equivalent to running decodeGOP's body
+ * (DVC_Decoder.cpp:39-435, without intraRecon and the deblocking filter) on
+ * each frame; replaces the ParallelMode 2/3 calls forwardME_CUDA,
+ * noiseDistribution_CUDA, condBitProb_CUDA, beliefPropagation_CUDA*,
+ * updateSI_CUDA and updateSMF_CUDA (forwardME_kernel.h:13,
+ * noiseModel_kernel.h:17-19, LDPCA_cuda.h:19-20, updateSI_kernel.h:16,
+ * motionLearning_kernel.h:13) together with the CPU stages between them. */
+int dvc_decode_wz_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames);
+
+/* dvc_decode_wz_frames on one frame that also returns intermediate stages for
+ * stage-level checks (each may be NULL): the side information after
+ * createSideInfo and the intra copy (DVC_Decoder.cpp:54-56), the noise
+ * parameters alpha (noiseParameter, :79) and the side information after the
+ * last updateSI (:318).  No counterpart in the reference. */
+int dvc_debug_wz_frame(dvc_ctx *ctx, dvc_wz_frame *frame, uint8_t *si_initial, float *alpha, uint8_t *si_final);
+
 #ifdef __cplusplus
 }
 #endif
