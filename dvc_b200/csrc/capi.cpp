@@ -281,3 +281,209 @@ static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t 
   }
   return DVC_OK;
 }
+
+// ---------------------------------------------------------------- sessions
+
+struct dvc_session {
+  dvc_ctx *ctx = nullptr;
+  int w = 0, h = 0, count = 0;
+  std::vector<dvc::DevBuf> ref, lp, ip, out;
+  std::vector<std::vector<uint8_t>> host_inputs;  // copies of mode/crc/acc for prepare
+  std::vector<dvc::FrameBatcher> batches;
+  std::vector<std::vector<int>> batch_frames;     // frame indices of each batch
+  std::vector<cudaStream_t> streams;
+  std::vector<std::vector<dvc::FrameResult>> results;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  std::vector<cudaEvent_t> done;
+  dvc::ProfileStats prof;
+  long long runs = 0;
+};
+
+static void session_release(dvc_session *S) {
+  for (auto &b : S->batches) b.release();
+  for (auto *v : {&S->ref, &S->lp, &S->ip, &S->out})
+    for (auto &b : *v) b.release();
+  for (cudaStream_t st : S->streams) cudaStreamDestroy(st);
+  for (cudaEvent_t e : S->done) cudaEventDestroy(e);
+  if (S->t0) cudaEventDestroy(S->t0);
+  if (S->t1) cudaEventDestroy(S->t1);
+}
+
+extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *frames, int max_batch, int nstreams,
+                                  dvc_session **out) {
+  if (!ctx || !out || count <= 0 || !frames) return DVC_E_ARG;
+  Context &c = ctx->c;
+  *out = nullptr;
+  if (max_batch <= 0) max_batch = count;
+  if (nstreams <= 0) nstreams = 1;
+  const int w = frames[0].width, h = frames[0].height;
+  for (int i = 0; i < count; i++) {
+    const dvc_wz_frame &f = frames[i];
+    if (f.width != w || f.height != h || !((w == 176 && h == 144) || (w == 352 && h == 288)) || f.qindex < 1 ||
+        f.qindex > 8 || !f.past || !f.future || !f.ac_range || !f.crc || !f.acc_synd || !f.recon) {
+      c.err = "dvc_session_create: bad frame " + std::to_string(i);
+      return DVC_E_ARG;
+    }
+  }
+  dvc_session *S = new (std::nothrow) dvc_session();
+  if (!S) return DVC_E_NOMEM;
+  S->ctx = ctx;
+  S->w = w;
+  S->h = h;
+  S->count = count;
+  const size_t fs = (size_t)w * h;
+  int st = DVC_OK;
+  auto bail = [&](int code) {
+    session_release(S);
+    delete S;
+    return code;
+  };
+  std::map<const uint8_t *, int> refs;
+  for (int i = 0; i < count; i++)
+    for (const uint8_t *p : {frames[i].past, frames[i].future})
+      if (!refs.count(p)) {
+        const int k = (int)refs.size();
+        refs[p] = k;
+      }
+  S->ref.resize(refs.size());
+  S->lp.resize(refs.size());
+  S->ip.resize(refs.size());
+  S->out.resize(count);
+  cudaStream_t s0 = c.stream;
+  for (auto &kv : refs) {
+    const int k = kv.second;
+    if (!S->ref[k].ensure(fs) || !S->lp[k].ensure(fs) || !S->ip[k].ensure(fs * 4)) {
+      c.err = "device allocation failed";
+      return bail(DVC_E_NOMEM);
+    }
+    if ((st = cuda_status(c, cudaMemcpyAsync(S->ref[k].p, kv.first, fs, cudaMemcpyHostToDevice, s0), "H2D ref")) ||
+        (st = cuda_status(c, dvc::launch_ref_planes(S->ref[k].as<uint8_t>(), w, h, S->lp[k].as<uint8_t>(),
+                                                    S->ip[k].as<uint8_t>(), s0),
+                          "reference planes")))
+      return bail(st);
+  }
+  for (int i = 0; i < count; i++) {
+    if (!S->out[i].ensure(fs)) {
+      c.err = "device allocation failed";
+      return bail(DVC_E_NOMEM);
+    }
+    if ((st = cuda_status(c, cudaMemcpyAsync(S->out[i].p, frames[i].recon, fs, cudaMemcpyHostToDevice, s0), "H2D")))
+      return bail(st);
+  }
+  if ((st = cuda_status(c, cudaStreamSynchronize(s0), "session upload"))) return bail(st);
+  for (int k = 0; k < nstreams; k++) {
+    cudaStream_t sk;
+    if ((st = cuda_status(c, cudaStreamCreateWithFlags(&sk, cudaStreamNonBlocking), "stream"))) return bail(st);
+    S->streams.push_back(sk);
+    cudaEvent_t e;
+    if ((st = cuda_status(c, cudaEventCreate(&e), "event"))) return bail(st);
+    S->done.push_back(e);
+  }
+  if ((st = cuda_status(c, cudaEventCreate(&S->t0), "event")) || (st = cuda_status(c, cudaEventCreate(&S->t1), "event")))
+    return bail(st);
+  const int nb = (count + max_batch - 1) / max_batch;
+  S->batches.resize(nb);
+  S->batch_frames.resize(nb);
+  S->results.resize(nb);
+  for (int b = 0; b < nb; b++) {
+    std::vector<dvc::FrameSpec> specs;
+    for (int i = b * max_batch; i < std::min(count, (b + 1) * max_batch); i++) {
+      const dvc_wz_frame &f = frames[i];
+      dvc::FrameSpec sp;
+      sp.w = w;
+      sp.h = h;
+      sp.qindex = f.qindex;
+      const int pr = refs[f.past], fr = refs[f.future];
+      sp.past = S->ref[pr].as<uint8_t>();
+      sp.future = S->ref[fr].as<uint8_t>();
+      sp.past_lp = S->lp[pr].as<uint8_t>();
+      sp.future_lp = S->lp[fr].as<uint8_t>();
+      sp.past_ip = S->ip[pr].as<uint8_t>();
+      sp.future_ip = S->ip[fr].as<uint8_t>();
+      sp.past_idx = f.past_idx;
+      sp.future_idx = f.future_idx;
+      sp.cur_idx = f.cur_idx;
+      sp.mode = f.mode;
+      sp.skip_mode = f.skip_mode;
+      sp.intra_mode = f.intra_mode;
+      for (int j = 0; j < 16; j++) sp.ac_range[j] = f.ac_range[j];
+      sp.crc = f.crc;
+      sp.acc = f.acc_synd;
+      sp.recon = S->out[i].as<uint8_t>();
+      specs.push_back(sp);
+      S->batch_frames[b].push_back(i);
+    }
+    cudaStream_t sb = S->streams[b % nstreams];
+    if (!S->batches[b].prepare(c, specs, sb)) return bail(DVC_E_CUDA);
+    if ((st = cuda_status(c, cudaStreamSynchronize(sb), "session prepare"))) return bail(st);
+  }
+  *out = S;
+  return DVC_OK;
+}
+
+extern "C" int dvc_session_run(dvc_session *S, int profile, double *elapsed_ms) {
+  if (!S) return DVC_E_ARG;
+  Context &c = S->ctx->c;
+  const int ns = (int)S->streams.size();
+  int st;
+  cudaStream_t s0 = S->streams[0];
+  if ((st = cuda_status(c, cudaEventRecord(S->t0, s0), "event"))) return st;
+  for (int k = 1; k < ns; k++)
+    if ((st = cuda_status(c, cudaStreamWaitEvent(S->streams[k], S->t0, 0), "wait"))) return st;
+  for (size_t b = 0; b < S->batches.size(); b++)
+    if (!S->batches[b].execute(c, S->streams[b % ns], 50, profile ? &S->prof : nullptr)) return DVC_E_CUDA;
+  for (int k = 1; k < ns; k++) {
+    if ((st = cuda_status(c, cudaEventRecord(S->done[k], S->streams[k]), "event"))) return st;
+    if ((st = cuda_status(c, cudaStreamWaitEvent(s0, S->done[k], 0), "wait"))) return st;
+  }
+  if ((st = cuda_status(c, cudaEventRecord(S->t1, s0), "event"))) return st;
+  for (size_t b = 0; b < S->batches.size(); b++)
+    if (!S->batches[b].collect(c, S->results[b], S->streams[b % ns])) return DVC_E_CUDA;
+  if ((st = cuda_status(c, cudaEventSynchronize(S->t1), "session run"))) return st;
+  if (profile)
+    for (auto &b : S->batches) b.harvest(&S->prof);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, S->t0, S->t1);
+  if (elapsed_ms) *elapsed_ms = ms;
+  S->runs++;
+  return DVC_OK;
+}
+
+extern "C" int dvc_session_frame(dvc_session *S, int index, uint8_t *recon, int *wz_bits, int *plane_results) {
+  if (!S || index < 0 || index >= S->count) return DVC_E_ARG;
+  Context &c = S->ctx->c;
+  for (size_t b = 0; b < S->batch_frames.size(); b++)
+    for (size_t j = 0; j < S->batch_frames[b].size(); j++)
+      if (S->batch_frames[b][j] == index) {
+        if (S->results[b].size() <= j) {
+          c.err = "dvc_session_frame: no completed run";
+          return DVC_E_ARG;
+        }
+        const dvc::FrameResult &r = S->results[b][j];
+        if (wz_bits) *wz_bits = r.wz_bits;
+        if (plane_results) memcpy(plane_results, r.planes.data(), r.planes.size() * sizeof(int));
+        if (recon) {
+          int st = cuda_status(c, cudaMemcpy(recon, S->out[index].p, (size_t)S->w * S->h, cudaMemcpyDeviceToHost),
+                               "D2H recon");
+          if (st) return st;
+        }
+        return DVC_OK;
+      }
+  return DVC_E_ARG;
+}
+
+extern "C" int dvc_session_profile(dvc_session *S, double *out5) {
+  if (!S || !out5) return DVC_E_ARG;
+  out5[0] = S->prof.ldpca_ms;
+  out5[1] = (double)S->prof.ldpca_launches;
+  out5[2] = (double)S->prof.ldpca_codewords;
+  out5[3] = (double)S->prof.kernel_launches;
+  out5[4] = (double)S->runs;
+  return DVC_OK;
+}
+
+extern "C" void dvc_session_destroy(dvc_session *S) {
+  if (!S) return;
+  session_release(S);
+  delete S;
+}

@@ -104,6 +104,8 @@ bool FrameBatcher::ensure_pinned(size_t b) {
 }
 
 void FrameBatcher::release() {
+  for (cudaEvent_t e : ev_) cudaEventDestroy(e);
+  ev_.clear();
   for (auto &s : slots_) s.release();
   slots_.clear();
   frames_dev_.release();
@@ -115,10 +117,9 @@ void FrameBatcher::release() {
 
 static size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
-bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, std::vector<FrameResult> &results,
-                          cudaStream_t s, int max_iter) {
+bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, cudaStream_t s) {
   const int nf = (int)frames.size();
-  results.assign(nf, FrameResult());
+  nf_ = 0;
   if (nf == 0) return true;
   const int w = frames[0].w, h = frames[0].h;
   const int n = w * h / 16, nb = n / 8, b8n = w * h / 64;
@@ -159,9 +160,6 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
   const size_t fd_off = pinned_need;
   pinned_need += align16(sizeof(FrameDev) * nf);
   // LDPCA steps: (band, bit) while any frame codes the band
-  struct Step {
-    int band, bit;
-  };
   std::vector<Step> steps;
   for (int band = 0; band < 16; band++) {
     int maxbits = 0;
@@ -183,6 +181,7 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
   uint8_t *pin = (uint8_t *)pinned_;
 
   if ((int)slots_.size() < nf) slots_.resize(nf);
+  wz_bits0_.assign(nf, 0);
   size_t off = 0;
   for (int f = 0; f < nf; f++) {
     const FrameSpec &F = frames[f];
@@ -213,7 +212,7 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
         D.crange[i] = 0;
       }
     }
-    results[f].wz_bits = wz_bits;
+    wz_bits0_[f] = wz_bits;
     for (int i = 0; i < 16; i++) {
       D.level_shift[i] = level_shift[i];
       D.qbits[i] = kQBits[q][i];
@@ -289,9 +288,6 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
       acc_planes += kQBits[q][kZigzag[band]];
     }
     if (!ctx.cuda_ok(cudaMemcpyAsync(S.in.p, P, p.total, cudaMemcpyHostToDevice, s), "H2D frame inputs")) return false;
-    if (!ctx.cuda_ok(cudaMemsetAsync(S.recons_trans.p, 0, (size_t)w * h * 4, s), "memset")) return false;
-    if (!ctx.cuda_ok(cudaMemsetAsync(D.dbf, 0, (size_t)w * h, s), "memset")) return false;
-    if (!ctx.cuda_ok(cudaMemsetAsync(S.alpha.p, 0, (size_t)w * h * 4, s), "memset")) return false;
     off += p.total;
   }
   FrameDev *fd_pin = (FrameDev *)(pin + fd_off);
@@ -334,6 +330,48 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
                    "H2D jobs"))
     return false;
 
+  steps_ = steps;
+  fd_ = fd;
+  qb_ = qb;
+  spec_copy_ = frames;
+  nf_ = nf;
+  w_ = w;
+  h_ = h;
+  max_nsir_ = max_nsir;
+  res_off_ = res_off;
+  L_ = L;
+  return true;
+}
+
+long long FrameBatcher::launches_per_execute() const {
+  if (nf_ == 0) return 0;
+  long long bands = 0;
+  for (size_t i = 0; i < steps_.size(); i++)
+    if (i == 0 || steps_[i].band != steps_[i - 1].band) bands++;
+  // side info 8, prep 6, per band 1 + 5, per step 2, final 1
+  return 8 + 6 + bands * 6 + (long long)steps_.size() * 2 + 1;
+}
+
+bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileStats *prof) {
+  if (nf_ == 0) return true;
+  const int nf = nf_, w = w_, h = h_, max_nsir = max_nsir_;
+  const std::vector<FrameDev> &fd = fd_;
+  const std::vector<FrameSpec> &frames = spec_copy_;
+  const std::vector<Step> &steps = steps_;
+  const LadderDev *L = L_;
+  FrameDev *fdev = frames_dev_.as<FrameDev>();
+  for (int f = 0; f < nf; f++) {
+    if (!ctx.cuda_ok(cudaMemsetAsync(fd[f].recons_trans, 0, (size_t)w * h * 4, s), "memset")) return false;
+    if (!ctx.cuda_ok(cudaMemsetAsync(fd[f].dbf, 0, (size_t)w * h, s), "memset")) return false;
+    if (!ctx.cuda_ok(cudaMemsetAsync(fd[f].alpha, 0, (size_t)w * h * 4, s), "memset")) return false;
+  }
+  ev_used_ = 0;
+  if (prof)
+    while (ev_.size() < 2 * steps.size()) {
+      cudaEvent_t e;
+      if (!ctx.cuda_ok(cudaEventCreate(&e), "event")) return false;
+      ev_.push_back(e);
+    }
   // ---- the decode
   if (!ctx.cuda_ok(launch_side_info(fdev, nf, w, h, s), "side information")) return false;
   if (!ctx.cuda_ok(launch_frame_prep(fdev, nf, w, h, s), "frame preparation")) return false;
@@ -354,8 +392,15 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
     for (; si < steps.size() && steps[si].band == band; si++) {
       if (!ctx.cuda_ok(launch_cond_bit(fdev, nf, w, h, band, steps[si].bit, s), "conditional bit probability"))
         return false;
+      if (prof) cudaEventRecord(ev_[ev_used_], s);
       if (!ctx.cuda_ok(launch_ldpca(*L, jobs_dev_.as<LdpcaJob>() + si * nf, nf, ctx.xlm, max_iter, s), "LDPCA"))
         return false;
+      if (prof) {
+        cudaEventRecord(ev_[ev_used_ + 1], s);
+        ev_used_ += 2;
+        prof->ldpca_launches++;
+        prof->ldpca_codewords += nf;
+      }
     }
     if (!ctx.cuda_ok(launch_band_end(fdev, nf, w, h, max_nsir, band, ctx.xlm, s), "band reconstruction")) return false;
   }
@@ -366,8 +411,23 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
                      "debug copy"))
       return false;
 
-  // ---- per-bitplane results
-  uint8_t *rp = pin + res_off;
+  if (prof) prof->kernel_launches += launches_per_execute();
+  return true;
+}
+
+void FrameBatcher::harvest(ProfileStats *prof) {
+  for (int i = 0; i + 1 < ev_used_; i += 2) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ev_[i], ev_[i + 1]) == cudaSuccess && prof) prof->ldpca_ms += ms;
+  }
+  ev_used_ = 0;
+}
+
+bool FrameBatcher::collect(Context &ctx, std::vector<FrameResult> &results, cudaStream_t s) {
+  const int nf = nf_;
+  results.assign(nf, FrameResult());
+  const std::vector<int> &qb = qb_;
+  uint8_t *rp = (uint8_t *)pinned_ + res_off_;
   size_t ro = 0;
   for (int f = 0; f < nf; f++) {
     if (!ctx.cuda_ok(cudaMemcpyAsync(rp + ro, slots_[f].out.p, (size_t)qb[f] * 20, cudaMemcpyDeviceToHost, s), "D2H"))
@@ -377,6 +437,7 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
   if (!ctx.cuda_ok(cudaStreamSynchronize(s), "decode")) return false;
   ro = 0;
   for (int f = 0; f < nf; f++) {
+    results[f].wz_bits = wz_bits0_[f];
     const int *r = (const int *)(rp + ro);
     const float *e = (const float *)(rp + ro + (size_t)qb[f] * 16);
     results[f].planes.assign(r, r + qb[f] * 4);
@@ -384,6 +445,15 @@ bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, st
     for (int p = 0; p < qb[f]; p++) results[f].wz_bits += r[4 * p];
     ro += (size_t)qb[f] * 20;
   }
+  return true;
+}
+
+bool FrameBatcher::decode(Context &ctx, const std::vector<FrameSpec> &frames, std::vector<FrameResult> &results,
+                          cudaStream_t s, int max_iter, ProfileStats *prof) {
+  results.clear();
+  if (frames.empty()) return true;
+  if (!(prepare(ctx, frames, s) && execute(ctx, s, max_iter, prof) && collect(ctx, results, s))) return false;
+  harvest(prof);
   return true;
 }
 

@@ -52,20 +52,51 @@ struct Slot {
   void release();
 };
 
+// Kernel-level measurements, filled while Context-level profiling is on.
+struct ProfileStats {
+  double ldpca_ms = 0;      // summed CUDA-event time of LDPCA ladder launches
+  long long ldpca_launches = 0, ldpca_codewords = 0, bp_iterations = 0;
+  long long kernel_launches = 0;  // every kernel this library launched
+};
+
 class FrameBatcher {
  public:
+  // prepare: per-frame constants, block lists, packed inputs, descriptors and
+  // LDPCA jobs, uploaded once; execute: the kernels only (no host transfer, no
+  // synchronisation); collect: per-bitplane results to the host.
+  bool prepare(Context &ctx, const std::vector<FrameSpec> &frames, cudaStream_t stream);
+  bool execute(Context &ctx, cudaStream_t stream, int max_iter = 50, ProfileStats *prof = nullptr);
+  bool collect(Context &ctx, std::vector<FrameResult> &results, cudaStream_t stream);
+  // after the stream has been synchronised: add the recorded LDPCA event times to prof
+  void harvest(ProfileStats *prof);
   bool decode(Context &ctx, const std::vector<FrameSpec> &frames, std::vector<FrameResult> &results,
-              cudaStream_t stream, int max_iter = 50);
+              cudaStream_t stream, int max_iter = 50, ProfileStats *prof = nullptr);
   void release();
   size_t slots() const { return slots_.size(); }
+  int frames() const { return nf_; }
+  // launches execute() issues (for the launch counter)
+  long long launches_per_execute() const;
 
  private:
   std::vector<Slot> slots_;
   DevBuf frames_dev_, jobs_dev_;
-  std::vector<uint8_t> staging_;
   void *pinned_ = nullptr;
   size_t pinned_bytes_ = 0;
   bool ensure_pinned(size_t b);
+  // prepared state
+  struct Step {
+    int band, bit;
+  };
+  std::vector<Step> steps_;
+  std::vector<FrameDev> fd_;
+  std::vector<int> qb_, wz_bits0_;
+  std::vector<const FrameSpec *> specs_;
+  std::vector<FrameSpec> spec_copy_;
+  int nf_ = 0, w_ = 0, h_ = 0, max_nsir_ = 0;
+  size_t res_off_ = 0;
+  const LadderDev *L_ = nullptr;
+  std::vector<cudaEvent_t> ev_;  // start/stop pairs of the LDPCA launches of one execute()
+  int ev_used_ = 0;
 };
 
 }  // namespace dvc

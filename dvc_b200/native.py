@@ -47,6 +47,8 @@ def lib():
             L.dvc_LdpcaDecoder.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.POINTER(C.c_int), C.c_ubyte, C.c_float]
             L.dvc_LdpcaDecoder.restype = C.c_int
+            L.dvc_session_destroy.argtypes = [C.c_void_p]
+            L.dvc_session_destroy.restype = None
             _declare_frame_api(L)
             _lib = L
     return _lib
@@ -74,6 +76,10 @@ class WZFrame(C.Structure):
 
 FRAME_API = {
     "dvc_decode_wz_frames": [C.c_void_p, C.c_int, C.POINTER(WZFrame)],
+    "dvc_session_create": [C.c_void_p, C.c_int, C.POINTER(WZFrame), C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+    "dvc_session_run": [C.c_void_p, C.c_int, C.POINTER(C.c_double)],
+    "dvc_session_frame": [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p],
+    "dvc_session_profile": [C.c_void_p, C.c_void_p],
     "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
@@ -142,6 +148,29 @@ class Context:
                                           C.c_ubyte(int(crc)), C.c_float(rate_lower_bound)))
         return dec, rate.value, lr
 
+    def _frame_array(self, items):
+        keep, arr, outs = [], (WZFrame * len(items))(), []
+        for i, it in enumerate(items):
+            w, h = it["width"], it["height"]
+            past = np.ascontiguousarray(it["past"], np.uint8)
+            fut = np.ascontiguousarray(it["future"], np.uint8)
+            mode = None if it.get("mode") is None else np.ascontiguousarray(it["mode"], np.uint8)
+            acr = np.ascontiguousarray(it["ac_range"], np.int32)
+            crc = np.ascontiguousarray(it["crc"], np.uint8)
+            acc = np.ascontiguousarray(it["acc"], np.uint8)
+            rec = np.zeros((h, w), np.uint8) if it.get("recon") is None else \
+                np.ascontiguousarray(it["recon"], np.uint8).copy()
+            keep += [past, fut, mode, acr, crc, acc, rec]
+            arr[i] = WZFrame(w, h, it["qindex"], it["past_idx"], it["future_idx"], it["cur_idx"], _ptr(past),
+                             _ptr(fut), _ptr(mode), it.get("skip_mode", 0), it.get("intra_mode", 0), _ptr(acr),
+                             _ptr(crc), _ptr(acc), _ptr(rec), 0, None, None, None)
+            outs.append(len(crc))
+        return arr, keep, outs
+
+    def session(self, items, max_batch=0, streams=1):
+        """Device-resident session over independent frames (dvc_session_*)."""
+        return Session(self, items, max_batch, streams)
+
     def debug_wz_frame(self, item):
         """One frame through dvc_debug_wz_frame: the decode result plus si_initial, alpha, si_final."""
         return self.decode_wz_frames([item], debug=True)[0]
@@ -188,3 +217,44 @@ class Context:
         for i, o in enumerate(outs):
             o["wz_bits"] = arr[i].wz_bits
         return outs
+
+
+class Session:
+    """dvc_session: inputs uploaded once, decoded on every run() from device memory."""
+
+    def __init__(self, ctx, items, max_batch=0, streams=1):
+        self.ctx = ctx
+        arr, keep, self.qbits = ctx._frame_array(items)
+        self.w, self.h = items[0]["width"], items[0]["height"]
+        self._h = C.c_void_p()
+        ctx.check(lib().dvc_session_create(ctx.handle, len(items), arr, max_batch, streams, C.byref(self._h)))
+        self.count = len(items)
+
+    def run(self, profile=False):
+        ms = C.c_double(0)
+        self.ctx.check(lib().dvc_session_run(self._h, 1 if profile else 0, C.byref(ms)))
+        return ms.value
+
+    def frame(self, i, recon=True):
+        rec = np.zeros((self.h, self.w), np.uint8) if recon else None
+        bits = C.c_int(0)
+        planes = np.zeros((self.qbits[i], 4), np.int32)
+        self.ctx.check(lib().dvc_session_frame(self._h, i, _ptr(rec), C.byref(bits), _ptr(planes)))
+        return rec, bits.value, planes
+
+    def profile(self):
+        out = np.zeros(5, np.float64)
+        self.ctx.check(lib().dvc_session_profile(self._h, _ptr(out)))
+        return dict(ldpca_ms=out[0], ldpca_launches=int(out[1]), ldpca_codewords=int(out[2]),
+                    kernel_launches=int(out[3]), runs=int(out[4]))
+
+    def close(self):
+        if self._h:
+            lib().dvc_session_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,47 @@
+"""Small, self-contained GPU workloads for profiler captures.
+
+    python -m dvc_b200.profile_cases ldpca-cif     # LDPCA ladder on the 11 CIF golden bitplanes
+    python -m dvc_b200.profile_cases frame-cif     # one CIF WZ frame (Q4) through every kernel
+
+Each case runs once after one warm-up run, so a profiler can skip the warm-up
+launches and capture the second instance of a kernel.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def ldpca_cif(ctx):
+    g = np.load(os.path.join(ROOT, "tests", "golden", "ldpca_cif.npz"))
+    for _ in range(2):
+        dec, res, ent = ctx.ldpca_decode(g["lr"], g["acc"], g["crc"])
+    assert np.array_equal(res[:, 0], g["rate"])
+
+
+def frame_cif(ctx):
+    from . import bitstream as bs, decoder, encoder, synth
+    ori, key = synth.make_sequence("cif", 3, 101)
+    st = bs.parse_wz(encoder.encode_sequence(ori, 2, 4))
+    m, b, e = bs.sequence_order(st.n_frames, st.gop)[0]
+    it = decoder.frame_item(st, st.frames[m], key)
+    for _ in range(2):
+        ctx.decode_wz_frames([it])
+
+
+CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif}
+
+
+def main():
+    from . import native
+    name = sys.argv[1] if len(sys.argv) > 1 else "ldpca-cif"
+    ctx = native.Context(0)
+    CASES[name](ctx)
+    ctx.close()
+    print("case", name, "done")
+
+
+if __name__ == "__main__":
+    main()

@@ -107,6 +107,27 @@ int dvc_decode_wz_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames);
  * last updateSI (:318).  No counterpart in the reference. */
 int dvc_debug_wz_frame(dvc_ctx *ctx, dvc_wz_frame *frame, uint8_t *si_initial, float *alpha, uint8_t *si_final);
 
+/* Device-resident decoding session: the frames' inputs and reference frames
+ * are uploaded once by dvc_session_create; every dvc_session_run decodes all
+ * of them again from device memory, in batches of at most `max_batch` frames
+ * spread over `streams` concurrent CUDA streams, and keeps the results on the
+ * device until dvc_session_frame copies them out.  Frames of one session must
+ * share one size and be independent of each other.  No counterpart in the
+ * reference (its GPU path copies every stage's data in and out). */
+typedef struct dvc_session dvc_session;
+int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *frames, int max_batch, int streams,
+                       dvc_session **out);
+/* Decode every frame of the session once; returns when the device is done.
+ * *elapsed_ms: device time of the whole run from CUDA events (may be NULL).
+ * profile != 0 also times each LDPCA launch (see dvc_session_profile). */
+int dvc_session_run(dvc_session *ses, int profile, double *elapsed_ms);
+/* Results of the last run for frame `index` (any output may be NULL). */
+int dvc_session_frame(dvc_session *ses, int index, uint8_t *recon, int *wz_bits, int *plane_results);
+/* Accumulated profile since creation: [0] LDPCA kernel ms, [1] LDPCA launches,
+ * [2] LDPCA codewords, [3] kernel launches, [4] runs. */
+int dvc_session_profile(dvc_session *ses, double *out5);
+void dvc_session_destroy(dvc_session *ses);
+
 #ifdef __cplusplus
 }
 #endif
