@@ -22,6 +22,7 @@ struct dvc_ctx {
 
 namespace dvc {
 cudaError_t launch_ref_planes(const uint8_t *recon, int w, int h, uint8_t *lp, uint8_t *ip, cudaStream_t s);
+Context *context_of(dvc_ctx *ctx) { return &ctx->c; }
 }
 
 using dvc::Context;

@@ -80,6 +80,8 @@ FRAME_API = {
     "dvc_session_run": [C.c_void_p, C.c_int, C.POINTER(C.c_double)],
     "dvc_session_frame": [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p],
     "dvc_session_profile": [C.c_void_p, C.c_void_p],
+    "dvc_ldpca_decode_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
@@ -137,6 +139,18 @@ class Context:
         self.check(lib().dvc_ldpca_decode(self._h, n, count, _ptr(lr), _ptr(acc), _ptr(crc), _ptr(dec), _ptr(res),
                                           _ptr(ent), max_iter))
         return dec, res, ent
+
+    def ldpca_decode_noalloc(self, n, count, d_lr, d_acc, d_crc, d_decoded, d_results, d_entropy, max_iter=50,
+                             stream=0):
+        """dvc_ldpca_decode_noalloc on caller-owned device buffers (integer device addresses);
+        enqueues on `stream` and returns without waiting. Returns the status code."""
+        return lib().dvc_ldpca_decode_noalloc(self._h, n, count, C.c_void_p(d_lr), C.c_void_p(d_acc),
+                                              C.c_void_p(d_crc), C.c_void_p(d_decoded) if d_decoded else None,
+                                              C.c_void_p(d_results), C.c_void_p(d_entropy) if d_entropy else None,
+                                              max_iter, C.c_void_p(stream) if stream else None)
+
+    def last_error(self):
+        return lib().dvc_last_error(self._h).decode()
 
     def LdpcaDecoder(self, lr, acc_bits, crc, rate_lower_bound):
         """Reference-shaped call: returns (decoded bits, rate, log LR)."""

@@ -107,6 +107,29 @@ int dvc_decode_wz_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames);
  * last updateSI (:318).  No counterpart in the reference. */
 int dvc_debug_wz_frame(dvc_ctx *ctx, dvc_wz_frame *frame, uint8_t *si_initial, float *alpha, uint8_t *si_final);
 
+/* Most codewords one dvc_ldpca_decode_noalloc call accepts. */
+#define DVC_NOALLOC_MAX_CODEWORDS 1024
+
+/* LDPCA ladder decode for callers that cannot allocate device memory at call
+ * time (cudaMalloc may synchronise the whole device, cannot run under stream
+ * capture, and fails when another framework's pool owns the memory).  Same
+ * results as dvc_ldpca_decode, but every buffer is the caller's device memory
+ * and the call only enqueues work on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream), returning before the device is done.  The
+ * per-codeword descriptors the kernel reads are kept in a fixed array in the
+ * library's device memory (DVC_NOALLOC_MAX_CODEWORDS entries, about 100 KB,
+ * held on every GPU that loads the library until the process exits); more
+ * codewords per call are rejected with DVC_E_ARG.  The first call on each
+ * device looks that array's address up, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race.
+ *   d_lr[count*n] f32, d_acc[count*n/8], d_crc[count]       inputs
+ *   d_decoded[count*n] (may be NULL), d_results[count*4],    outputs
+ *   d_entropy[count] (may be NULL)
+ * No counterpart in the reference. */
+int dvc_ldpca_decode_noalloc(dvc_ctx *ctx, int n, int count, const float *d_lr, const uint8_t *d_acc,
+                             const uint8_t *d_crc, uint8_t *d_decoded, int *d_results, float *d_entropy,
+                             int max_iter, void *stream);
+
 /* Device-resident decoding session: the frames' inputs and reference frames
  * are uploaded once by dvc_session_create; every dvc_session_run decodes all
  * of them again from device memory, in batches of at most `max_batch` frames
