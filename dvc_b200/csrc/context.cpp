@@ -2,7 +2,10 @@
 #include "context.h"
 
 #include <stdio.h>
+#include <stdlib.h>
 #include <sys/stat.h>
+
+#include "kernels.h"
 
 namespace dvc {
 
@@ -42,6 +45,7 @@ bool Context::init(const char *data, const char *tables, int dev) {
   mkdir(table_dir.c_str(), 0755);
   if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return false;
   if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
+  if (const char *nt = getenv("DVC_LDPCA_THREADS")) set_ldpca_threads(atoi(nt));
 
   // library-exact math tables: load, or sweep the C library once and cache
   const std::string xpath = table_dir + "/xlm_tables.bin";
@@ -60,8 +64,16 @@ bool Context::init(const char *data, const char *tables, int dev) {
     return true;
   };
   if (!up(xlm_host.log_tab, &xlm.log_tab) || !up(xlm_host.exp_tab, &xlm.exp_tab) ||
-      !up(xlm_host.em1_bitmap, &xlm.em1_bitmap))
+      !up(xlm_host.em1_bitmap, &xlm.em1_bitmap) || !up(xlm_host.esc_tab, &xlm.esc_tab))
     return fail("uploading libm tables failed");
+  {
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(XlmSmallTables)) != cudaSuccess) return fail("uploading libm tables failed");
+    xlm_allocs.push_back(p);
+    if (cudaMemcpy(p, &xlm_host.small, sizeof(XlmSmallTables), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail("uploading libm tables failed");
+    xlm.small = (const XlmSmallTables *)p;
+  }
   auto lg2 = [](uint32_t v) {
     int s = 0;
     while ((1u << s) < v) s++;
@@ -71,6 +83,9 @@ bool Context::init(const char *data, const char *tables, int dev) {
   xlm.exp_mask = xlm_host.hdr.exp_cap - 1;
   xlm.log_shift = 32 - lg2(xlm_host.hdr.log_cap);
   xlm.exp_shift = 32 - lg2(xlm_host.hdr.exp_cap);
+  // no escapes: skip the escape lookup entirely
+  xlm.esc_mask = xlm_host.hdr.esc_count ? xlm_host.hdr.esc_cap - 1 : 0;
+  xlm.esc_shift = 32 - lg2(xlm_host.hdr.esc_cap);
   xlm.tanh_ylo = xlm_host.hdr.tanh_ylo;
   xlm.tanh_y1 = xlm_host.hdr.tanh_y1;
 

@@ -2,7 +2,9 @@
 //
 // All float/double arithmetic in these kernels is compiled with -fmad=false so
 // that every product and sum is rounded separately, as in the reference's x86
-// SSE2 build; divisions and square roots are IEEE (no fast-math).
+// SSE2 build; divisions and square roots are IEEE (no fast-math).  The only
+// fused multiply-adds are the explicit ones of the table-driven exp/log in
+// exact_libm.h, which the host table builder evaluates the same way.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -12,8 +14,7 @@
 
 namespace dvc {
 
-// zig-zag band order and quantiser tables (DvcDec/src/global.cpp:36-41,
-// reconstruction.cpp:9-78)
+// zig-zag band order (DvcDec/src/global.cpp:36-41)
 __constant__ int c_zigzag[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
 
 #define DVC_WZ_B 0
@@ -23,58 +24,78 @@ __constant__ int c_zigzag[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 1
 // ------------------------------------------------------------------------
 // Library-exact float functions (see exact_libm.h for the method).
 
+// view of the small tables in global memory
+__device__ __forceinline__ XlSmall xl_small_global(const XlmDev &t) {
+  return XlSmall{t.small->exp2j, t.small->invc, t.small->logc, t.small->efold};
+}
+
+// copy the small tables into shared memory (every thread of the block calls
+// this; follow with __syncthreads); `buf` holds sizeof(XlmSmallTables) bytes
+__device__ __forceinline__ XlSmall xl_small_stage(const XlmDev &t, XlmSmallTables *buf) {
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(t.small);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(buf);
+  for (int i = threadIdx.x; i < (int)(sizeof(XlmSmallTables) / 4); i += blockDim.x) dst[i] = src[i];
+  return XlSmall{buf->exp2j, buf->invc, buf->logc, buf->efold};
+}
+
 __device__ __forceinline__ float xl_hash_lookup(const uint32_t *tab, uint32_t mask, int shift, uint32_t key,
                                                 float fallback) {
   uint32_t s = (key * 0x9E3779B1u) >> shift;
+  uint2 kv = __ldg(reinterpret_cast<const uint2 *>(tab + 2 * s));
+  if (kv.x == key) return __uint_as_float(kv.y);
   // load factor <= 1/2, so an empty slot ends every probe; the bound is a guard
-  for (uint32_t probe = 0; probe <= mask; probe++) {
-    const uint2 kv = *reinterpret_cast<const uint2 *>(tab + 2 * s);
-    if (kv.x == key) return __uint_as_float(kv.y);
-    if (kv.x == 0xFFFFFFFFu) break;
+  for (uint32_t probe = 0; kv.x != 0xFFFFFFFFu && probe < mask; probe++) {
     s = (s + 1) & mask;
+    kv = __ldg(reinterpret_cast<const uint2 *>(tab + 2 * s));
+    if (kv.x == key) return __uint_as_float(kv.y);
   }
   return fallback;
 }
 
 // logf as the C library computes it, for every positive float up to 10001
-__device__ __forceinline__ float xl_logf(const XlmDev &t, float x) {
+__device__ __forceinline__ float xl_logf(const XlmDev &t, const XlSmall &s, float x) {
   const uint32_t u = __float_as_uint(x);
   if (!(x > 0.0f) || u >= 0x7f800000u) {
     if (x == 0.0f) return __uint_as_float(0xff800000u);  // -inf
     if (u == 0x7f800000u) return x;                      // +inf
     return __uint_as_float(0x7fc00000u);                 // NaN
   }
-  const float m = xl_logf_base(x);
+  const float m = xl_logf_base(x, s);
   if (u > XL_LOG_HI) return m;
   return xl_hash_lookup(t.log_tab, t.log_mask, t.log_shift, u, m);
 }
 
 // expf as the C library computes it, for x <= 0
-__device__ __forceinline__ float xl_expf(const XlmDev &t, float x) {
+__device__ __forceinline__ float xl_expf(const XlmDev &t, const XlSmall &s, float x) {
   const uint32_t u = __float_as_uint(x);
   if (x != x) return x;
   if (u >= XL_EXP_HI && (u >> 31)) return 0.0f;  // x <= -104 (and -inf): underflows to +0
-  const float m = xl_expf_base(x);
+  const float m = xl_expf_base(x, s);
   if (!(u >> 31)) return m;  // positive arguments do not occur in the decoder
   return xl_hash_lookup(t.exp_tab, t.exp_mask, t.exp_shift, u, m);
 }
 
 // tanhf as the C library computes it, for y >= 2^-31
-__device__ __forceinline__ float xl_tanhf(const XlmDev &t, float y) {
+__device__ __forceinline__ float xl_tanhf(const XlmDev &t, const XlSmall &s, float y) {
   const uint32_t u = __float_as_uint(y);
-  if (u >= t.tanh_y1) return 1.0f;     // also NaN/negative patterns, which the decoder never forms
-  if (u < t.tanh_ylo) return y;        // below every argument the decoder forms; keeps the bitmap read in range
+  if (u >= t.tanh_y1) return 1.0f;  // also NaN/negative patterns, which the decoder never forms
+  if (u < t.tanh_ylo) return y;     // below every argument the decoder forms; keeps the bitmap read in range
   const bool big = y >= 1.0f;
   const float a = big ? __fmul_rn(2.0f, y) : __fmul_rn(-2.0f, y);
-  const double d = xl_expm1_d((double)a);
+  const double d = xl_expm1_d((double)a, s);
   float e = __double2float_rn(d);
   const uint32_t i = u - t.tanh_ylo;
-  if ((t.em1_bitmap[i >> 5] >> (i & 31)) & 1u) e = xl_step_toward(e, d);
+  if ((__ldg(t.em1_bitmap + (i >> 5)) >> (i & 31)) & 1u) {
+    const float st = xl_step_toward(e, d);
+    e = t.esc_mask ? xl_hash_lookup(t.esc_tab, t.esc_mask, t.esc_shift, u, st) : st;
+  }
   const float den = __fadd_rn(e, 2.0f);
   return big ? __fsub_rn(1.0f, __fdiv_rn(2.0f, den)) : __fdiv_rn(-e, den);
 }
 
 // -log(tanh(y)) with the reference's two library calls (LdpcaDecoder.cpp:513,519)
-__device__ __forceinline__ float xl_phi(const XlmDev &t, float y) { return -xl_logf(t, xl_tanhf(t, y)); }
+__device__ __forceinline__ float xl_phi(const XlmDev &t, const XlSmall &s, float y) {
+  return -xl_logf(t, s, xl_tanhf(t, s, y));
+}
 
 }  // namespace dvc

@@ -45,4 +45,12 @@ struct LdpcaJob {
   int w, index_in_blk;
 };
 
+// Scratch of the speculative ladder form (k_ldpca.cu): per codeword the lowest
+// successful code, summed BP iterations and first code; per (codeword, block)
+// the code it succeeded with and its decoded bits.
+struct LdpcaSpec {
+  int *best = nullptr, *iters = nullptr, *start = nullptr, *slot_code = nullptr;
+  uint8_t *slot_dec = nullptr;
+};
+
 }  // namespace dvc

@@ -8,22 +8,29 @@
 // return the same bits as that library for every input the decoder can feed.
 //
 // Method (two parts):
-//  1. xl_*_d: double-precision evaluations written here from standard
-//     mathematics, using only IEEE-rounded +, -, *, / (no fused multiply-add,
-//     no library calls), so host and device produce identical bits:
-//       exp:   Cody-Waite reduction x = k*ln2 + r (ln2 split into a 44-bit head
-//              and a tail), Taylor series of e^r to r^13, scaled by 2^k;
-//       log:   x = 2^e * m with m in [sqrt(1/2), sqrt(2)), s = (m-1)/(m+1),
-//              log m = 2 atanh(s) = 2s(1 + s^2/3 + s^4/5 + ... + s^22/23);
-//       expm1: Taylor series to a^18 for |a| < 1/2, else exp(a) - 1.
+//  1. xl_*_d: double-precision evaluations written here from the table-driven
+//     method of P. T. P. Tang ("Table-driven implementation of the exponential
+//     function", ACM TOMS 15(2), 1989; "... of the logarithm function", ACM TOMS
+//     16(4), 1990), using only IEEE-rounded operations and explicit fused
+//     multiply-adds, so host and device produce identical bits:
+//       exp:   x = (32k + j) ln2/32 + r, |r| <= ln2/64; e^x = 2^k * T[j] * P(r)
+//              with T[j] = 2^(j/32) and P the degree-6 Taylor polynomial;
+//       expm1: degree-9 Taylor polynomial for |a| < 2^-5, else exp(a) - 1;
+//       log:   x = 2^e * m, m in [1, 2) split into 128 bins; per bin a
+//              reciprocal centre 1/c and log c (bins at and above sqrt 2 fold
+//              into [sqrt(1/2), 1) so that values near 1 keep full relative
+//              accuracy), log x = (e + f) ln2 + log c + log1p(m/c - 1) with a
+//              degree-8 polynomial for log1p.
+//     The small tables are computed on the host at table-build time and stored
+//     with the correction tables, so host and device always use the same ones.
 //     Rounding the double result to float gives the correctly rounded value
 //     except in rare near-tie cases.
 //  2. Correction tables built on the host by sweeping the C library over the
 //     exact input domain (libm_tables.cpp): the inputs where the library's float
-//     result differs from part 1, with the library's value.  The library's
-//     errors stay below one ulp, so its result is always the float neighbour of
-//     part 1's on the side of the double value; for expm1f this lets a plain
-//     bitmap mark the exceptions.  The builder verifies this for every input.
+//     result differs from part 1, with the library's value.  For expm1f a bitmap
+//     marks the exceptions; the library's value is then the float neighbour on
+//     the side of part 1's double value, except for a few inputs kept in a
+//     small escape hash.  The builder verifies this for every input.
 //
 // tanhf is not swept directly: over the whole decoder domain the library's
 // tanhf(y) equals, bit for bit, 1 - 2/(expm1f(2y)+2) for y >= 1 and
@@ -31,6 +38,7 @@
 // exactly 1 from a threshold y1 upward.  The builder checks this identity for
 // every y in the domain before writing any table.
 #pragma once
+#include <math.h>
 #include <stdint.h>
 
 #if defined(__CUDACC__)
@@ -40,33 +48,26 @@
 #endif
 
 #if defined(__CUDA_ARCH__)
-#define XL_DMUL(a, b) __dmul_rn((a), (b))
-#define XL_DADD(a, b) __dadd_rn((a), (b))
-#define XL_DSUB(a, b) __dsub_rn((a), (b))
-#define XL_DDIV(a, b) __ddiv_rn((a), (b))
-#define XL_FADD(a, b) __fadd_rn((a), (b))
-#define XL_FSUB(a, b) __fsub_rn((a), (b))
-#define XL_FMUL(a, b) __fmul_rn((a), (b))
-#define XL_FDIV(a, b) __fdiv_rn((a), (b))
+#define XL_FMA(a, b, c) __fma_rn((a), (b), (c))
 #define XL_D2F(a) __double2float_rn(a)
 #else
-#define XL_DMUL(a, b) ((a) * (b))
-#define XL_DADD(a, b) ((a) + (b))
-#define XL_DSUB(a, b) ((a) - (b))
-#define XL_DDIV(a, b) ((a) / (b))
-#define XL_FADD(a, b) ((a) + (b))
-#define XL_FSUB(a, b) ((a) - (b))
-#define XL_FMUL(a, b) ((a) * (b))
-#define XL_FDIV(a, b) ((a) / (b))
+#define XL_FMA(a, b, c) fma((a), (b), (c))
 #define XL_D2F(a) ((float)(a))
 #endif
 
-// ln 2 = XL_LN2_HI + XL_LN2_LO; the head has 44 significant bits so k*head is
-// exact for |k| < 2^9.
+// ln 2 = XL_LN2_HI + XL_LN2_LO (44-bit head)
 #define XL_LN2_HI 0x1.62e42fefa38p-1
 #define XL_LN2_LO 0x1.ef35793c7673p-45
 #define XL_INV_LN2 0x1.71547652b82fep+0
-#define XL_SQRT2 0x1.6a09e667f3bcdp+0
+
+// the small tables of part 1 (host copies live in libm_tables.cpp; device copies
+// are read through this view, from global or shared memory)
+struct XlSmall {
+  const double *exp2j;  // [32] 2^(j/32)
+  const double *invc;   // [128] reciprocal bin centre
+  const double *logc;   // [128] log of the centre, folded bins minus ln 2
+  const int *efold;     // [128] 1 for bins folded into [sqrt(1/2), 1)
+};
 
 XL_HD uint64_t xl_dbits(double d) {
   union { double d; uint64_t u; } c;
@@ -89,95 +90,67 @@ XL_HD float xl_bitsf(uint32_t u) {
   return c.f;
 }
 
-// round-half-away of |v| < 2^31 without library calls (the sign of ties does
-// not matter for the reduction, only host/device agreement does)
-XL_HD int xl_round_int(double v) { return (int)(v >= 0.0 ? XL_DADD(v, 0.5) : XL_DSUB(v, 0.5)); }
-
-// e^x for x in [-745, 709]; used on [-110, 20].
-XL_HD double xl_exp_d(double x) {
-  const int k = xl_round_int(XL_DMUL(x, XL_INV_LN2));
+// e^x for x in [-745, 88]; the decoder uses [-110, 20]
+XL_HD double xl_exp_d(double x, const XlSmall &s) {
+  const double t = x * (32.0 * XL_INV_LN2);
+  const int k = (int)(t >= 0.0 ? t + 0.5 : t - 0.5);
   const double kd = (double)k;
-  const double r = XL_DSUB(XL_DSUB(x, XL_DMUL(kd, XL_LN2_HI)), XL_DMUL(kd, XL_LN2_LO));
-  double p = 1.0 / 6227020800.0;          // 1/13!
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 479001600.0);  // 1/12!
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 39916800.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 3628800.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 362880.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 40320.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 5040.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 720.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 120.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 24.0);
-  p = XL_DADD(XL_DMUL(p, r), 1.0 / 6.0);
-  p = XL_DADD(XL_DMUL(p, r), 0.5);
-  // e^r = 1 + r + r^2 p
-  const double er = XL_DADD(1.0, XL_DADD(r, XL_DMUL(XL_DMUL(r, r), p)));
-  // 2^k as a double (k in [-1022, 1023] here; two steps keep it normal)
-  const int k1 = k / 2, k2 = k - k1;
-  const double s1 = xl_bitsd((uint64_t)(k1 + 1023) << 52);
-  const double s2 = xl_bitsd((uint64_t)(k2 + 1023) << 52);
-  return XL_DMUL(XL_DMUL(er, s1), s2);
+  double r = XL_FMA(-kd, XL_LN2_HI / 32.0, x);
+  r = XL_FMA(-kd, XL_LN2_LO / 32.0, r);
+  double q = 1.0 / 720.0;
+  q = XL_FMA(q, r, 1.0 / 120.0);
+  q = XL_FMA(q, r, 1.0 / 24.0);
+  q = XL_FMA(q, r, 1.0 / 6.0);
+  q = XL_FMA(q, r, 0.5);
+  q = XL_FMA(q, r, 1.0);
+  const double er = XL_FMA(q, r, 1.0);
+  const int j = k & 31, hi = (k - j) / 32;
+  // 2^hi in two normal factors
+  const int h1 = hi / 2, h2 = hi - h1;
+  const double s1 = xl_bitsd((uint64_t)(h1 + 1023) << 52), s2 = xl_bitsd((uint64_t)(h2 + 1023) << 52);
+  return ((s.exp2j[j] * er) * s1) * s2;
 }
 
 // e^a - 1 for a in [-2, 20]
-XL_HD double xl_expm1_d(double a) {
-  if (a > -0.5 && a < 0.5) {
-    double q = 1.0 / 6402373705728000.0;  // 1/18!
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 355687428096000.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 20922789888000.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 1307674368000.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 87178291200.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 6227020800.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 479001600.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 39916800.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 3628800.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 362880.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 40320.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 5040.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 720.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 120.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 24.0);
-    q = XL_DADD(XL_DMUL(q, a), 1.0 / 6.0);
-    q = XL_DADD(XL_DMUL(q, a), 0.5);
-    // a + a^2 q
-    return XL_DADD(a, XL_DMUL(XL_DMUL(a, a), q));
+XL_HD double xl_expm1_d(double a, const XlSmall &s) {
+  if (a > -0.03125 && a < 0.03125) {
+    double q = 1.0 / 362880.0;
+    q = XL_FMA(q, a, 1.0 / 40320.0);
+    q = XL_FMA(q, a, 1.0 / 5040.0);
+    q = XL_FMA(q, a, 1.0 / 720.0);
+    q = XL_FMA(q, a, 1.0 / 120.0);
+    q = XL_FMA(q, a, 1.0 / 24.0);
+    q = XL_FMA(q, a, 1.0 / 6.0);
+    q = XL_FMA(q, a, 0.5);
+    return XL_FMA(a * a, q, a);
   }
-  return XL_DSUB(xl_exp_d(a), 1.0);
+  return xl_exp_d(a, s) - 1.0;
 }
 
-// natural log of a positive normal double
-XL_HD double xl_log_d(double x) {
+// natural log of a positive double that came from a float (normal as a double)
+XL_HD double xl_log_d(double x, const XlSmall &s) {
   const uint64_t u = xl_dbits(x);
-  int e = (int)((u >> 52) & 0x7ff) - 1023;
-  double m = xl_bitsd((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull);  // [1, 2)
-  if (m > XL_SQRT2) {
-    m = XL_DMUL(m, 0.5);
-    e += 1;
-  }
-  const double s = XL_DDIV(XL_DSUB(m, 1.0), XL_DADD(m, 1.0));
-  const double z = XL_DMUL(s, s);
-  double q = 1.0 / 23.0;
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 21.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 19.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 17.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 15.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 13.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 11.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 9.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 7.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 5.0);
-  q = XL_DADD(XL_DMUL(q, z), 1.0 / 3.0);
-  const double s2 = XL_DADD(s, s);
-  // log m = 2s + 2s z q
-  const double lm = XL_DADD(s2, XL_DMUL(XL_DMUL(s2, z), q));
-  const double ed = (double)e;
-  return XL_DADD(XL_DMUL(ed, XL_LN2_HI), XL_DADD(lm, XL_DMUL(ed, XL_LN2_LO)));
+  const int e = (int)((u >> 52) & 0x7ff) - 1023;
+  const double m = xl_bitsd((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull);  // [1, 2)
+  const int i = (int)((u >> 45) & 127);
+  const double r = XL_FMA(m, s.invc[i], -1.0);
+  double q = -1.0 / 8.0;
+  q = XL_FMA(q, r, 1.0 / 7.0);
+  q = XL_FMA(q, r, -1.0 / 6.0);
+  q = XL_FMA(q, r, 1.0 / 5.0);
+  q = XL_FMA(q, r, -1.0 / 4.0);
+  q = XL_FMA(q, r, 1.0 / 3.0);
+  q = XL_FMA(q, r, -0.5);
+  const double l1p = XL_FMA(r * r, q, r);
+  const double ed = (double)(e + s.efold[i]);
+  const double head = XL_FMA(ed, XL_LN2_HI, s.logc[i]);
+  return head + XL_FMA(ed, XL_LN2_LO, l1p);
 }
 
 // float results of part 1, before corrections
-XL_HD float xl_expf_base(float x) { return XL_D2F(xl_exp_d((double)x)); }
-XL_HD float xl_expm1f_base(float a) { return XL_D2F(xl_expm1_d((double)a)); }
-XL_HD float xl_logf_base(float x) { return XL_D2F(xl_log_d((double)x)); }
+XL_HD float xl_expf_base(float x, const XlSmall &s) { return XL_D2F(xl_exp_d((double)x, s)); }
+XL_HD float xl_expm1f_base(float a, const XlSmall &s) { return XL_D2F(xl_expm1_d((double)a, s)); }
+XL_HD float xl_logf_base(float x, const XlSmall &s) { return XL_D2F(xl_log_d((double)x, s)); }
 
 // the float neighbour of r on the side of the double value d (d != r)
 XL_HD float xl_step_toward(float r, double d) {

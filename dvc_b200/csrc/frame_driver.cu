@@ -12,7 +12,10 @@
 #include "frame_driver.h"
 
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
+
+#include <algorithm>
 
 #include "kernels.h"
 
@@ -330,6 +333,15 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
                    "H2D jobs"))
     return false;
 
+  // speculative ladder width: spread each codeword over idle SMs when the batch is small
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
+    int k = sms / std::max(1, nf);
+    if (const char *e = getenv("DVC_LDPCA_SPEC")) k = atoi(e);
+    spec_k_ = std::max(1, std::min(8, k));
+    if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_))) return ctx.fail("device allocation failed");
+  }
   steps_ = steps;
   fd_ = fd;
   qb_ = qb;
@@ -348,8 +360,8 @@ long long FrameBatcher::launches_per_execute() const {
   long long bands = 0;
   for (size_t i = 0; i < steps_.size(); i++)
     if (i == 0 || steps_[i].band != steps_[i - 1].band) bands++;
-  // side info 8, prep 6, per band 1 + 5, per step 2, final 1
-  return 8 + 6 + bands * 6 + (long long)steps_.size() * 2 + 1;
+  // side info 8, prep 6, per band 1 + 5, per step condBitProb + ladder + finalize, final 1
+  return 8 + 6 + bands * 6 + (long long)steps_.size() * 3 + 1;
 }
 
 bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileStats *prof) {
@@ -393,7 +405,9 @@ bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileSt
       if (!ctx.cuda_ok(launch_cond_bit(fdev, nf, w, h, band, steps[si].bit, s), "conditional bit probability"))
         return false;
       if (prof) cudaEventRecord(ev_[ev_used_], s);
-      if (!ctx.cuda_ok(launch_ldpca(*L, jobs_dev_.as<LdpcaJob>() + si * nf, nf, ctx.xlm, max_iter, s), "LDPCA"))
+      if (!ctx.cuda_ok(launch_ldpca_spec(*L, jobs_dev_.as<LdpcaJob>() + si * nf, nf, ctx.xlm, max_iter, spec_k_,
+                                         ldpca_spec_carve(spec_.p, nf, spec_k_), s),
+                       "LDPCA"))
         return false;
       if (prof) {
         cudaEventRecord(ev_[ev_used_ + 1], s);

@@ -79,7 +79,8 @@ class FrameBatcher {
 
  private:
   std::vector<Slot> slots_;
-  DevBuf frames_dev_, jobs_dev_;
+  DevBuf frames_dev_, jobs_dev_, spec_;
+  int spec_k_ = 1;
   void *pinned_ = nullptr;
   size_t pinned_bytes_ = 0;
   bool ensure_pinned(size_t b);

@@ -628,11 +628,12 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
   __shared__ float prob[ML_N];
   __shared__ int sc[ML_N];
   __shared__ int s_n, s_dmax;
+  const XlSmall xs = xl_small_global(xt);
   float *out = F.pdf + (size_t)s_idx * F.pdf_stride;
   if (index == 0) {
     const float a = F.alpha[top * w + left];
     const int s = F.oct[((size_t)top * srw + left) * 16];
-    for (int k = threadIdx.x; k < range; k += NT) out[k] = xl_expf(xt, -a * (float)abs(k - s));
+    for (int k = threadIdx.x; k < range; k += NT) out[k] = xl_expf(xt, xs, -a * (float)abs(k - s));
     return;
   }
   const float a = F.alpha[(top + (index >> 2)) * w + left + (index & 3)];
@@ -653,7 +654,7 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
   __syncthreads();
   const int nm = s_n, dmax = s_dmax;
   const int tab = dmax < NOISE_TAB ? dmax + 1 : NOISE_TAB;
-  for (int d = threadIdx.x; d < tab; d += NT) etab[d] = xl_expf(xt, -a * (float)d);
+  for (int d = threadIdx.x; d < tab; d += NT) etab[d] = xl_expf(xt, xs, -a * (float)d);
   __syncthreads();
   const int rmax = 2 * range + 1;
   for (int k = threadIdx.x; k < rmax; k += NT) {
@@ -661,7 +662,7 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
     float sum = 0.0f;
     for (int m = 0; m < nm; m++) {
       const int d = abs(pc - sc[m]);
-      const float e = d < NOISE_TAB ? etab[d] : xl_expf(xt, -a * (float)d);
+      const float e = d < NOISE_TAB ? etab[d] : xl_expf(xt, xs, -a * (float)d);
       sum += prob[m] * e;
     }
     out[k] = sum;
@@ -891,6 +892,7 @@ __global__ void update_smf_kernel(FrameDev *frames, XlmDev xt, int band) {
   const int top = (blk / b4w) << 2, left = (blk % b4w) << 2;
   const Win wn = ml_window(top, left, w, h);
   const int cw = wn.sr - wn.sl + 1, nc = cw * (wn.sb - wn.st + 1);
+  const XlSmall xs = xl_small_global(xt);
   float *p = F.smf + (size_t)warp * ML_N;
   float pr[3];
   for (int r = 0; r < 3; r++) {
@@ -904,7 +906,7 @@ __global__ void update_smf_kernel(FrameDev *frames, XlmDev xt, int band) {
           const float d = (float)F.recon[(top + ii) * w + left + jj] - (float)F.si[(m + ii) * w + n + jj];
           sse += d * d;
         }
-      pr[r] = xl_expf(xt, (float)-0.01f * sse);
+      pr[r] = xl_expf(xt, xs, (float)-0.01f * sse);
     }
   }
   // sequential sum in candidate order

@@ -1,8 +1,8 @@
-// LDPCA rate-adaptive decoding on the device: one thread block per codeword
-// runs the whole request ladder (start code from the conditional-entropy bound,
-// syndrome of each ladder code from the accumulated syndrome, sum-product belief
-// propagation with the parity early stop, CRC-8 acceptance, and the GF(2)
-// inverse at full rate) with no host round trip between requests.
+// LDPCA rate-adaptive decoding on the device: the whole request ladder (start
+// code from the conditional-entropy bound, syndrome of each ladder code from the
+// accumulated syndrome, sum-product belief propagation with the parity early
+// stop, CRC-8 acceptance, and the GF(2) inverse at full rate) with no host round
+// trip between requests.
 //
 // Reference: DvcDec/src/LdpcaDecoder.cpp LdpcaDecoder (:646-771),
 // beliefPropagation (:462-580), ComputeCE (:127-143), invH_mul (:624-643).
@@ -11,14 +11,23 @@
 // library functions (logf, tanhf via exact_libm) follow the reference exactly,
 // so decoded bits, accepted codes and rates are identical to it.
 //
-// Shared-memory layout per codeword (n bits, e edges; CIF n=6336, e=19008):
-//   msg[e] f32   the single edge-message array, updated in place:
-//                v->c message -> phi(|v->c|) -> c->v message -> next v->c
-//   llr[n] f32   log(p0/p1)
-//   rowt[n] f32  row sums of phi (m <= n rows)
-//   sgn[e/32]    sign bits of the v->c messages
-//   dec[n], synd[n], acc[n] u8  (synd bit 1 holds the row sign parity during BP)
-// CIF: 148 KB, one block per SM; QCIF: 37 KB.
+// Two launch forms share one kernel:
+//  * direct (K = 1, no scratch): one thread block per codeword walks the ladder
+//    code by code, exactly as the reference does;
+//  * speculative (K >= 1, scratch): K blocks per codeword try the ladder codes
+//    start+k, start+k+K, ... concurrently.  A code is accepted by the reference
+//    iff BP converges and the CRC matches and no lower code was accepted, i.e.
+//    the accepted code is the lowest code that succeeds; blocks publish
+//    successes with atomicMin, stop at (or abandon) codes above the best success
+//    so far, and ldpca_finalize_kernel picks the lowest success (or the
+//    full-rate inverse when none), so results are identical to the sequential
+//    ladder while idle SMs shorten it.
+//
+// Shared memory per codeword (n bits, e edges; CIF n=6336, e=19008), ~167 KB CIF:
+//   msg[e] f32  edge messages, in place: phi(|v->c|) -> c->v -> next phi(|v->c|)
+//   sg8[e] u8   sign of each v->c message
+//   llr[n], rowt[n] f32; dec[n], synd[n] (bit 1: row sign parity), acc[n] u8;
+//   the small exp/log tables of exact_libm.
 #include <cuda_runtime.h>
 
 #include "dvc_common.cuh"
@@ -28,225 +37,389 @@
 namespace dvc {
 
 #define LDPCA_LOG2 (0.693147181f)  // LdpcaDecoder.cpp:18
+#define LDPCA_NONE 0x7f7f7f7f      // "no success yet" (memset pattern 0x7f)
 
 static __host__ __device__ size_t ldpca_smem_bytes(int n, int e) {
-  size_t b = 0;
-  b += (size_t)e * 4;                  // msg
-  b += (size_t)n * 4;                  // llr
-  b += (size_t)n * 4;                  // rowt
-  b += (size_t)((e + 31) / 32) * 4;    // sgn
-  b += (size_t)n * 3;                  // dec, synd, acc
+  size_t b = sizeof(XlmSmallTables);
+  b += (size_t)e * 4;   // msg
+  b += (size_t)n * 4;   // llr
+  b += (size_t)n * 4;   // rowt
+  b += (size_t)e;       // sg8
+  b += (size_t)n * 3;   // dec, synd, acc
   return (b + 15) & ~(size_t)15;
 }
 
 size_t ldpca_smem_size(int n, int e) { return ldpca_smem_bytes(n, e); }
 
+// fused bitplane insertion (putBitplaneToCoeff, bitplane.cpp:4-22)
+__device__ __forceinline__ void put_bitplane(const LdpcaJob &J, const uint8_t *dec, int n) {
+  const int b4w = J.w >> 2, b8w = J.w >> 3;
+  const int row = J.index_in_blk >> 2, col = J.index_in_blk & 3;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const int i = k / b4w, j = k - i * b4w;
+    if (J.mode[(i >> 1) * b8w + (j >> 1)] == DVC_WZ_B) {
+      int *p = J.recons_trans + ((i << 2) + row) * J.w + (j << 2) + col;
+      *p = (*p << 1) + (int)dec[k];
+    }
+  }
+}
+
+// decoded = inv(H) * syndrome of the full-rate code (LdpcaDecoder.cpp:695-716);
+// syndrome words are built in `sw` (n/32 words of shared memory)
+__device__ void invh_decode(const LadderDev &L, const uint8_t *synd, uint8_t *dec, uint32_t *sw) {
+  const int n = L.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nt = blockDim.x;
+  for (int base = warp * 32; base < n; base += nt) {
+    const int k = base + lane;
+    const uint32_t b = __ballot_sync(0xffffffffu, k < n && (synd[k] & 1));
+    if (lane == 0) sw[base >> 5] = b;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < n; j += nt) {
+    const uint32_t *row = L.invh + (size_t)j * L.invh_words;
+    uint32_t x = 0;
+    for (int w = 0; w < L.invh_words; w++) x ^= __ldg(row + w) & sw[w];
+    dec[j] = (uint8_t)(__popc(x) & 1);
+  }
+  __syncthreads();
+}
+
+// syndrome of ladder code `code` from the accumulated syndrome bits (LdpcaDecoder.cpp:684-693)
+__device__ __forceinline__ void build_syndrome(const LadderDev &L, int code, const uint8_t *acc, uint8_t *synd) {
+  const int m = L.synd_len[code], nb = L.bpp[code];
+  const int *idx = L.idx + (size_t)code * L.period;
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    uint8_t s = acc[idx[k % nb] + (k / nb) * L.period];
+    if (k > 0) s ^= acc[idx[(k - 1) % nb] + ((k - 1) / nb) * L.period];
+    synd[k] = s;
+  }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 1)
-    ldpca_ladder_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, XlmDev xt, int max_iter) {
+    ldpca_ladder_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, XlmDev xt, int max_iter, int K,
+                        LdpcaSpec sp) {
   extern __shared__ __align__(16) uint8_t smem[];
-  const LdpcaJob J = jobs[blockIdx.x];
+  const int j = blockIdx.x / K, kk = blockIdx.x - j * K;
+  const LdpcaJob J = jobs[j];
   if (!J.active) return;
+  const bool spec = sp.best != nullptr;
   const int n = L.n, E = L.e, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float *msg = reinterpret_cast<float *>(smem);
+  XlmSmallTables *tabs = reinterpret_cast<XlmSmallTables *>(smem);
+  float *msg = reinterpret_cast<float *>(smem + sizeof(XlmSmallTables));
   float *llr = msg + E;
   float *rowt = llr + n;
-  uint32_t *sgn = reinterpret_cast<uint32_t *>(rowt + n);
-  uint8_t *dec = reinterpret_cast<uint8_t *>(sgn + (E + 31) / 32);
+  uint8_t *sg8 = reinterpret_cast<uint8_t *>(rowt + n);
+  uint8_t *dec = sg8 + E;
   uint8_t *synd = dec + n;
   uint8_t *acc = synd + n;
   __shared__ uint32_t s_ured[NT / 32];
-  __shared__ int s_start, s_accepted;
-  __shared__ float s_entropy;
+  __shared__ int s_start, s_accepted, s_stop;
+  const XlSmall xs = xl_small_stage(xt, tabs);
+  __syncthreads();
 
-  // accumulated syndrome bits (ByteToBit, LdpcaDecoder.cpp:81-107) and the
-  // entropy terms (ComputeCE): H = sum_k (P(-log P + log(1-P)) - log(1-P)) / LOG2, P = LR/(1+LR)
+  // accumulated syndrome bits (ByteToBit, LdpcaDecoder.cpp:81-107), entropy
+  // terms H_k = (P(-log P + log(1-P)) - log(1-P)) / LOG2 with P = LR/(1+LR)
+  // (ComputeCE), and log LR (LdpcaDecoder.cpp:665-666)
   for (int k = tid; k < n; k += NT) {
     acc[k] = (uint8_t)((J.acc[k >> 3] >> (7 - (k & 7))) & 1);
     const float lr = J.lr[k];
     const float pco = lr / (1.0f + lr);
-    const float tmp = xl_logf(xt, 1.0f - pco);
-    msg[k] = (pco * (-xl_logf(xt, pco) + tmp) - tmp) / LDPCA_LOG2;
-    llr[k] = xl_logf(xt, lr);  // LdpcaDecoder.cpp:665-666
-    if (J.llr_out) J.llr_out[k] = llr[k];
+    const float tmp = xl_logf(xt, xs, 1.0f - pco);
+    msg[k] = (pco * (-xl_logf(xt, xs, pco) + tmp) - tmp) / LDPCA_LOG2;
+    llr[k] = xl_logf(xt, xs, lr);
+    if (J.llr_out && kk == 0) J.llr_out[k] = llr[k];
   }
   __syncthreads();
   if (tid == 0) {
     // the bound is a sequential float sum in block order
     float h = 0.0f;
-    for (int k = 0; k < n; k++) h += msg[k];
+    int k = 0;
+    for (; k + 8 <= n; k += 8) {
+      const float v0 = msg[k], v1 = msg[k + 1], v2 = msg[k + 2], v3 = msg[k + 3];
+      const float v4 = msg[k + 4], v5 = msg[k + 5], v6 = msg[k + 6], v7 = msg[k + 7];
+      h += v0;
+      h += v1;
+      h += v2;
+      h += v3;
+      h += v4;
+      h += v5;
+      h += v6;
+      h += v7;
+    }
+    for (; k < n; k++) h += msg[k];
     h /= (float)n;
     if (J.use_given_entropy) h = J.given_entropy;
     int start = 0;
     while (start < L.num_codes - 1 && L.code_rate[start] < h) start++;
-    s_entropy = h;
     s_start = start;
     s_accepted = L.num_codes - 1;
+    if (kk == 0) {
+      if (J.entropy) *J.entropy = h;
+      if (spec) sp.start[j] = start;
+    }
   }
   __syncthreads();
   const int start = s_start;
+  const int last = L.num_codes - 1;
   int total_iters = 0;
+  volatile int *bestp = spec ? sp.best + j : nullptr;
 
-  for (int code = start; code < L.num_codes; code++) {
+  for (int code = start + kk; code < last; code += K) {
+    if (spec) {
+      if (tid == 0) s_stop = *bestp < code;
+      __syncthreads();
+      if (s_stop) break;
+    }
     const int m = L.synd_len[code];
-    const int nb = L.bpp[code];
-    const int *idx = L.idx + (size_t)code * L.period;
-    // syndrome of this code: differences of the accumulated syndrome at the
-    // kept positions (LdpcaDecoder.cpp:684-693)
-    for (int k = tid; k < m; k += NT) {
-      const int cur = idx[k % nb] + (k / nb) * L.period;
-      uint8_t s = acc[cur];
-      if (k > 0) s ^= acc[idx[(k - 1) % nb] + ((k - 1) / nb) * L.period];
-      synd[k] = s;
-    }
-    __syncthreads();
-
-    if (m == n) {
-      // full rate: decoded = inv(H) * syndrome over GF(2) (LdpcaDecoder.cpp:695-716)
-      uint32_t *sw = sgn;  // reuse: n/32 syndrome words
-      for (int base = warp * 32; base < n; base += NT) {
-        const int k = base + lane;
-        const uint32_t b = __ballot_sync(0xffffffffu, k < n && synd[k]);
-        if (lane == 0) sw[base >> 5] = b;
-      }
-      __syncthreads();
-      for (int j = tid; j < n; j += NT) {
-        const uint32_t *row = L.invh + (size_t)j * L.invh_words;
-        uint32_t x = 0;
-        for (int w = 0; w < L.invh_words; w++) x ^= row[w] & sw[w];
-        dec[j] = (uint8_t)(__popc(x) & 1);
-      }
-      __syncthreads();
-      if (tid == 0) s_accepted = code;
-      break;
-    }
-
-    // ---- belief propagation (beliefPropagation, LdpcaDecoder.cpp:462-580)
+    build_syndrome(L, code, acc, synd);
     const int *rp = L.row_ptr + (size_t)code * (n + 1);
     const uint16_t *re = L.row_edge + (size_t)code * E;
     const uint16_t *ir = L.ir + (size_t)code * E;
-    for (int e = tid; e < E; e += NT) msg[e] = llr[L.edge_col[e]];
+    // first magnitudes: phi(|LLR|) on every edge of each column
+    for (int k = tid; k < n; k += NT) {
+      const float v = llr[k];
+      const bool neg = (__float_as_uint(v) >> 31) != 0;
+      const float y = ((neg ? -v : v) + 1e-9f) / 2.0f;
+      const float ph = xl_phi(xt, xs, y);
+      for (int e = L.jc[k]; e < L.jc[k + 1]; e++) {
+        msg[e] = ph;
+        sg8[e] = neg;
+      }
+    }
     __syncthreads();
     bool converged = false;
     int it = 0;
-    for (; it < max_iter && !converged; it++) {
-      // (1) sign and magnitude of every v->c message; phi of the magnitude
-      for (int base = warp * 32; base < E; base += NT) {
-        const int e = base + lane;
-        bool neg = false;
-        if (e < E) {
-          const float v = msg[e];
-          neg = (__float_as_uint(v) >> 31) != 0;
-          const float mag = neg ? -v : v;
-          msg[e] = xl_phi(xt, (mag + 1e-9f) / 2.0f);
-        }
-        const uint32_t b = __ballot_sync(0xffffffffu, neg);
-        if (lane == 0) sgn[base >> 5] = b;
-      }
-      __syncthreads();
-      // (2) per row: sum of phi in edge order, sign parity incl. the syndrome
+    while (it < max_iter) {
+      it++;
+      // (1) rows: sum of phi in edge order, sign parity including the syndrome
       for (int r = tid; r < m; r += NT) {
         float s = 0.0f;
         uint32_t par = synd[r] & 1u;
-        for (int p = rp[r]; p < rp[r + 1]; p++) {
+        const int p1 = rp[r + 1];
+        for (int p = rp[r]; p < p1; p++) {
           const int e = re[p];
           s += msg[e];
-          par ^= (sgn[e >> 5] >> (e & 31)) & 1u;
+          par ^= sg8[e];
         }
         rowt[r] = s;
-        synd[r] = (uint8_t)((synd[r] & 1u) | (par << 1));  // bit 1: sign parity of the row
+        synd[r] = (uint8_t)((synd[r] & 1u) | (par << 1));
       }
       __syncthreads();
-      // (3) c->v messages: phi(row sum - own phi) with the product of the other signs
-      for (int e = tid; e < E; e += NT) {
-        const int r = ir[e];
-        const float c = xl_phi(xt, (rowt[r] - msg[e] + 1e-9f) / 2.0f);
-        const uint32_t neg = ((uint32_t)synd[r] >> 1) ^ ((sgn[e >> 5] >> (e & 31)) & 1u);
-        msg[e] = c * (neg ? -1.0f : 1.0f);
+      // (2) edges: c->v = phi(row sum - own phi) with the product of the other signs
+      for (int e0 = tid; e0 < E; e0 += 2 * NT) {
+        const int e1 = e0 + NT;
+        const int r0 = __ldg(ir + e0);
+        const float y0 = (rowt[r0] - msg[e0] + 1e-9f) / 2.0f;
+        float y1 = 1.0f;
+        int r1 = 0;
+        if (e1 < E) {
+          r1 = __ldg(ir + e1);
+          y1 = (rowt[r1] - msg[e1] + 1e-9f) / 2.0f;
+        }
+        const float c0 = xl_phi(xt, xs, y0);
+        const float c1 = xl_phi(xt, xs, y1);
+        msg[e0] = c0 * ((((uint32_t)synd[r0] >> 1) ^ sg8[e0]) ? -1.0f : 1.0f);
+        if (e1 < E) msg[e1] = c1 * ((((uint32_t)synd[r1] >> 1) ^ sg8[e1]) ? -1.0f : 1.0f);
       }
       __syncthreads();
-      // (4) per column: total in edge order, extrinsic messages, hard decision
+      // (3) columns: total in edge order, hard decision, extrinsic messages and
+      //     their phi for the next iteration
       for (int k = tid; k < n; k += NT) {
-        const int e0 = L.jc[k], e1 = L.jc[k + 1];
+        const int ea = L.jc[k], eb = L.jc[k + 1];
         float tmp = llr[k];
-        for (int e = e0; e < e1; e++) tmp += msg[e];
-        for (int e = e0; e < e1; e++) msg[e] = tmp - msg[e];
+        for (int e = ea; e < eb; e++) tmp += msg[e];
         dec[k] = (uint8_t)(__float_as_uint(tmp) >> 31);
+        if (eb - ea == 3) {
+          const float v0 = tmp - msg[ea], v1 = tmp - msg[ea + 1], v2 = tmp - msg[ea + 2];
+          const bool n0 = (__float_as_uint(v0) >> 31) != 0, n1 = (__float_as_uint(v1) >> 31) != 0,
+                     n2 = (__float_as_uint(v2) >> 31) != 0;
+          const float p0 = xl_phi(xt, xs, ((n0 ? -v0 : v0) + 1e-9f) / 2.0f);
+          const float p1 = xl_phi(xt, xs, ((n1 ? -v1 : v1) + 1e-9f) / 2.0f);
+          const float p2 = xl_phi(xt, xs, ((n2 ? -v2 : v2) + 1e-9f) / 2.0f);
+          msg[ea] = p0;
+          msg[ea + 1] = p1;
+          msg[ea + 2] = p2;
+          sg8[ea] = n0;
+          sg8[ea + 1] = n1;
+          sg8[ea + 2] = n2;
+        } else {
+          for (int e = ea; e < eb; e++) {
+            const float v = tmp - msg[e];
+            const bool ng = (__float_as_uint(v) >> 31) != 0;
+            msg[e] = xl_phi(xt, xs, ((ng ? -v : v) + 1e-9f) / 2.0f);
+            sg8[e] = ng;
+          }
+        }
       }
       __syncthreads();
-      // (5) parity check of every row
+      // (4) parity check of every row; abandon a code above a known success
       int wrong = 0;
       for (int r = tid; r < m; r += NT) {
         uint32_t par = synd[r] & 1u;
-        for (int p = rp[r]; p < rp[r + 1]; p++) par ^= dec[L.edge_col[re[p]]];
+        const int p1 = rp[r + 1];
+        for (int p = rp[r]; p < p1; p++) par ^= dec[__ldg(L.edge_col + re[p])];
         wrong |= (int)par;
       }
+      if (spec && tid == 0) s_stop = *bestp < code;
       converged = __syncthreads_or(wrong) == 0;
+      if (converged || (spec && s_stop)) break;
     }
     total_iters += it;
-    // restore the plain syndrome bits (bit 1 held the row sign parity)
     for (int k = tid; k < m; k += NT) synd[k] &= 1u;
     __syncthreads();
-    if (converged) {
-      // CRC-8 of the decoded bitplane as the xor of single-bit CRCs
-      uint32_t c = 0;
-      for (int k = tid; k < n; k += NT)
-        if (dec[k]) c ^= L.crc_tab[k];
-      for (int o = 16; o > 0; o >>= 1) c ^= __shfl_xor_sync(0xffffffffu, c, o);
-      if (lane == 0) s_ured[warp] = c;
-      __syncthreads();
-      if (tid == 0) {
-        uint32_t t = 0;
-        for (int w = 0; w < NT / 32; w++) t ^= s_ured[w];
-        s_ured[0] = t;
-      }
-      __syncthreads();
-      const bool ok = (int)(s_ured[0] & 0xffu) == J.crc;
-      __syncthreads();
-      if (ok) {
-        if (tid == 0) s_accepted = code;
-        break;
-      }
+    if (!converged) continue;
+    // CRC-8 of the decoded bitplane as the xor of single-bit CRCs (the CRC is
+    // linear for a fixed length with zero initial value and no final xor)
+    uint32_t c = 0;
+    for (int k = tid; k < n; k += NT)
+      if (dec[k]) c ^= __ldg(L.crc_tab + k);
+    for (int o = 16; o > 0; o >>= 1) c ^= __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) s_ured[warp] = c;
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < NT / 32; w++) t ^= s_ured[w];
+      s_ured[0] = t;
     }
+    __syncthreads();
+    const bool ok = (int)(s_ured[0] & 0xffu) == J.crc;
+    __syncthreads();
+    if (ok) {
+      if (tid == 0) s_accepted = code;
+      if (spec) {
+        uint8_t *slot = sp.slot_dec + (size_t)blockIdx.x * n;
+        for (int k = tid; k < n; k += NT) slot[k] = dec[k];
+        __syncthreads();
+        if (tid == 0) {
+          sp.slot_code[blockIdx.x] = code;
+          __threadfence();
+          atomicMin(sp.best + j, code);
+        }
+      }
+      break;
+    }
+  }
+  if (spec) {
+    if (tid == 0) atomicAdd(sp.iters + j, total_iters);
+    return;
   }
   __syncthreads();
   const int accepted = s_accepted;
+  if (accepted == last) {
+    build_syndrome(L, last, acc, synd);
+    __syncthreads();
+    invh_decode(L, synd, dec, reinterpret_cast<uint32_t *>(msg));
+  }
   if (tid == 0) {
     J.result[0] = L.synd_len[accepted] + 8;
     J.result[1] = start;
     J.result[2] = accepted;
     J.result[3] = total_iters;
-    if (J.entropy) *J.entropy = s_entropy;
   }
   if (J.decoded)
     for (int k = tid; k < n; k += NT) J.decoded[k] = dec[k];
-  if (J.recons_trans) {
-    // putBitplaneToCoeff (bitplane.cpp:4-22): append the bit to WZ blocks' indices
-    const int b4w = J.w >> 2, b8w = J.w >> 3;
-    const int row = J.index_in_blk >> 2, col = J.index_in_blk & 3;
-    for (int k = tid; k < n; k += NT) {
-      const int i = k / b4w, j = k - i * b4w;
-      if (J.mode[(i >> 1) * b8w + (j >> 1)] == DVC_WZ_B) {
-        int *p = J.recons_trans + ((i << 2) + row) * J.w + (j << 2) + col;
-        *p = (*p << 1) + (int)dec[k];
-      }
-    }
-  }
+  if (J.recons_trans) put_bitplane(J, dec, n);
 }
 
-cudaError_t launch_ldpca(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
-                         int max_iter, cudaStream_t stream) {
-  if (num_jobs <= 0) return cudaSuccess;
-  constexpr int NT = 1024;
+// Speculative form: pick the lowest successful code (or the full-rate inverse
+// when no code below it succeeded) and write the outputs.
+__global__ void __launch_bounds__(256) ldpca_finalize_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, int K,
+                                                             LdpcaSpec sp) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int j = blockIdx.x;
+  const LdpcaJob J = jobs[j];
+  if (!J.active) return;
+  const int n = L.n, last = L.num_codes - 1;
+  uint32_t *sw = reinterpret_cast<uint32_t *>(smem);
+  uint8_t *acc = smem + (size_t)((n + 31) / 32) * 4, *synd = acc + n, *dec = synd + n;
+  const int best = sp.best[j];
+  const uint8_t *src = nullptr;
+  int accepted = last;
+  if (best != LDPCA_NONE && best < last) {
+    for (int k = 0; k < K; k++)
+      if (sp.slot_code[j * K + k] == best) src = sp.slot_dec + (size_t)(j * K + k) * n;
+    accepted = best;
+  }
+  if (src) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) dec[k] = src[k];
+    __syncthreads();
+  } else {
+    accepted = last;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) acc[k] = (uint8_t)((J.acc[k >> 3] >> (7 - (k & 7))) & 1);
+    __syncthreads();
+    build_syndrome(L, last, acc, synd);
+    __syncthreads();
+    invh_decode(L, synd, dec, sw);
+  }
+  if (threadIdx.x == 0) {
+    J.result[0] = L.synd_len[accepted] + 8;
+    J.result[1] = sp.start[j];
+    J.result[2] = accepted;
+    J.result[3] = sp.iters[j];
+  }
+  if (J.decoded)
+    for (int k = threadIdx.x; k < n; k += blockDim.x) J.decoded[k] = dec[k];
+  if (J.recons_trans) put_bitplane(J, dec, n);
+}
+
+template <int NT>
+static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_jobs, const XlmDev &xt, int max_iter,
+                             int K, const LdpcaSpec &sp, cudaStream_t stream) {
   const size_t smem = ldpca_smem_bytes(L.n, L.e);
   static bool attr_done = false;
   if (!attr_done) {
-    cudaError_t e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         200 * 1024);
+    cudaError_t e =
+        cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     if (e != cudaSuccess) return e;
     attr_done = true;
   }
-  ldpca_ladder_kernel<NT><<<num_jobs, NT, smem, stream>>>(L, jobs_dev, xt, max_iter);
+  ldpca_ladder_kernel<NT><<<num_jobs * K, NT, smem, stream>>>(L, jobs, xt, max_iter, K, sp);
+  return cudaGetLastError();
+}
+
+static int g_ldpca_threads = 1024;
+
+void set_ldpca_threads(int nt) { g_ldpca_threads = (nt == 512) ? 512 : 1024; }
+
+cudaError_t launch_ldpca(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt, int max_iter,
+                         cudaStream_t stream) {
+  if (num_jobs <= 0) return cudaSuccess;
+  LdpcaSpec none{};
+  return g_ldpca_threads == 512 ? launch_nt<512>(L, jobs_dev, num_jobs, xt, max_iter, 1, none, stream)
+                                : launch_nt<1024>(L, jobs_dev, num_jobs, xt, max_iter, 1, none, stream);
+}
+
+size_t ldpca_spec_scratch_bytes(int n, int num_jobs, int K) {
+  return (size_t)num_jobs * 12 + (size_t)num_jobs * K * 4 + (size_t)num_jobs * K * n + 64;
+}
+
+LdpcaSpec ldpca_spec_carve(void *base, int num_jobs, int K) {
+  LdpcaSpec sp;
+  uint8_t *p = (uint8_t *)base;
+  sp.best = (int *)p;
+  p += (size_t)num_jobs * 4;
+  sp.iters = (int *)p;
+  p += (size_t)num_jobs * 4;
+  sp.start = (int *)p;
+  p += (size_t)num_jobs * 4;
+  sp.slot_code = (int *)p;
+  p += (size_t)num_jobs * K * 4;
+  sp.slot_dec = p;
+  return sp;
+}
+
+cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
+                              int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream) {
+  if (num_jobs <= 0) return cudaSuccess;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(sp.best, 0x7f, (size_t)num_jobs * 4, stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(sp.iters, 0, (size_t)num_jobs * 4, stream)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(sp.slot_code, 0xff, (size_t)num_jobs * K * 4, stream)) != cudaSuccess) return e;
+  e = g_ldpca_threads == 512 ? launch_nt<512>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream)
+                             : launch_nt<1024>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+  if (e != cudaSuccess) return e;
+  const size_t fsmem = (size_t)((L.n + 31) / 32) * 4 + (size_t)3 * L.n;
+  ldpca_finalize_kernel<<<num_jobs, 256, fsmem, stream>>>(L, jobs_dev, K, sp);
   return cudaGetLastError();
 }
 

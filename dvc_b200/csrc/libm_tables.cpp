@@ -33,6 +33,30 @@ namespace {
 
 struct Pair { uint32_t key, val; };
 
+// Small tables of the table-driven base functions (exact_libm.h), computed in
+// extended precision: 2^(j/32); per mantissa bin of [1, 2) (128 bins) the
+// reciprocal of the bin centre and the log of the centre.  The bins touching 1
+// (the first) and 2 (the last, folded) use the exact centres 1 and 2.
+void make_small(XlmSmallTables &t) {
+  for (int j = 0; j < 32; j++) t.exp2j[j] = (double)exp2l((long double)j / 32.0L);
+  const long double sqrt2 = sqrtl(2.0L), ln2 = logl(2.0L);
+  for (int i = 0; i < 128; i++) {
+    long double c = 1.0L + ((long double)i + 0.5L) / 128.0L;
+    if (i == 0) c = 1.0L;
+    if (i == 127) c = 2.0L;
+    const double invc = (double)(1.0L / c);
+    const int fold = c >= sqrt2 ? 1 : 0;
+    t.invc[i] = invc;
+    t.efold[i] = fold;
+    // log of the exact reciprocal actually used, so log m = -log(invc) + log1p(m*invc - 1)
+    long double lc = -logl((long double)invc);
+    if (fold) lc -= ln2;
+    t.logc[i] = (double)lc;
+  }
+}
+
+XlSmall view(const XlmSmallTables &t) { return XlSmall{t.exp2j, t.invc, t.logc, t.efold}; }
+
 int hw_threads() {
   unsigned n = std::thread::hardware_concurrency();
   return n ? (int)n : 4;
@@ -78,13 +102,16 @@ float tanh_formula(float y, float e) {
 extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errlen) {
   if (threads <= 0) threads = hw_threads();
   std::vector<std::vector<Pair>> parts(threads);
+  XlmSmallTables small;
+  make_small(small);
+  const XlSmall sv = view(small);
 
   // ---- logf over (0, 10001]
   parallel_ranges(XL_LOG_LO, XL_LOG_HI, threads, [&](int t, uint64_t a, uint64_t b) {
     auto &v = parts[t];
     for (uint64_t u = a; u <= b; u++) {
       const float x = xl_bitsf((uint32_t)u);
-      const float g = logf(x), m = xl_logf_base(x);
+      const float g = logf(x), m = xl_logf_base(x, sv);
       if (xl_fbits(g) != xl_fbits(m)) v.push_back({(uint32_t)u, xl_fbits(g)});
     }
   });
@@ -96,7 +123,7 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
     auto &v = parts[t];
     for (uint64_t u = a; u <= b; u++) {
       const float x = xl_bitsf((uint32_t)u);
-      const float g = expf(x), m = xl_expf_base(x);
+      const float g = expf(x), m = xl_expf_base(x, sv);
       if (xl_fbits(g) != xl_fbits(m)) v.push_back({(uint32_t)u, xl_fbits(g)});
     }
   });
@@ -122,11 +149,12 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
   const uint32_t ylo = XL_TANH_YLO;
   const uint64_t ny = (uint64_t)y1 - ylo;
   std::vector<uint32_t> bitmap((ny + 31) / 32, 0u);
-  std::atomic<long long> bad_identity(0), bad_dir(0), em1_count(0);
+  std::atomic<long long> bad_identity(0), em1_count(0);
   std::atomic<uint32_t> first_bad(0);
+  std::vector<std::vector<Pair>> esc_parts(threads);
   // threads write disjoint 32-aligned word ranges
   const uint64_t words = bitmap.size();
-  parallel_ranges(0, words - 1, threads, [&](int, uint64_t wa, uint64_t wb) {
+  parallel_ranges(0, words - 1, threads, [&](int tid, uint64_t wa, uint64_t wb) {
     long long cnt = 0;
     for (uint64_t wi = wa; wi <= wb; wi++) {
       uint32_t word = 0;
@@ -136,12 +164,10 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
         const float y = xl_bitsf((uint32_t)(ylo + i));
         const float a = (y >= 1.0f) ? 2.0f * y : -2.0f * y;
         const float g = expm1f(a);
-        const float m = xl_expm1f_base(a);
+        const float m = xl_expm1f_base(a, sv);
         if (xl_fbits(g) != xl_fbits(m)) {
-          if (xl_fbits(xl_step_toward(m, xl_expm1_d((double)a))) != xl_fbits(g)) {
-            bad_dir++;
-            first_bad = ylo + (uint32_t)i;
-          }
+          if (xl_fbits(xl_step_toward(m, xl_expm1_d((double)a, sv))) != xl_fbits(g))
+            esc_parts[tid].push_back({ylo + (uint32_t)i, xl_fbits(g)});
           word |= 1u << bit;
           cnt++;
         }
@@ -154,16 +180,18 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
     }
     em1_count += cnt;
   });
-  if (bad_identity.load() || bad_dir.load()) {
-    snprintf(err, errlen, "tanh identity failures %lld, expm1f direction failures %lld (first y bits %08x)",
-             bad_identity.load(), bad_dir.load(), first_bad.load());
+  if (bad_identity.load()) {
+    snprintf(err, errlen, "tanh identity failures %lld (first y bits %08x)", bad_identity.load(), first_bad.load());
     return -3;
   }
+  std::vector<Pair> escp;
+  for (auto &v : esc_parts) escp.insert(escp.end(), v.begin(), v.end());
 
-  std::vector<uint32_t> log_tab, exp_tab;
-  uint32_t log_cap = 0, exp_cap = 0;
+  std::vector<uint32_t> log_tab, exp_tab, esc_tab;
+  uint32_t log_cap = 0, exp_cap = 0, esc_cap = 0;
   build_hash(logp, log_tab, log_cap);
   build_hash(expp, exp_tab, exp_cap);
+  build_hash(escp, esc_tab, esc_cap);
 
   XlmHeader h;
   memset(&h, 0, sizeof h);
@@ -177,6 +205,8 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
   h.tanh_y1 = y1;
   h.em1_words = (uint32_t)bitmap.size();
   h.em1_count = (uint32_t)em1_count.load();
+  h.esc_cap = esc_cap;
+  h.esc_count = (uint32_t)escp.size();
   std::string tmp = std::string(path) + ".tmp";
   FILE *f = fopen(tmp.c_str(), "wb");
   if (!f) {
@@ -187,6 +217,8 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
   fwrite(log_tab.data(), 4, log_tab.size(), f);
   fwrite(exp_tab.data(), 4, exp_tab.size(), f);
   fwrite(bitmap.data(), 4, bitmap.size(), f);
+  fwrite(esc_tab.data(), 4, esc_tab.size(), f);
+  fwrite(&small, sizeof small, 1, f);
   fclose(f);
   if (rename(tmp.c_str(), path) != 0) {
     snprintf(err, errlen, "cannot rename %s", tmp.c_str());
@@ -216,9 +248,12 @@ int dvc_libm_load(const char *path, XlmHost *out, char *err, int errlen) {
   out->log_tab.resize((size_t)h.log_cap * 2);
   out->exp_tab.resize((size_t)h.exp_cap * 2);
   out->em1_bitmap.resize(h.em1_words);
+  out->esc_tab.resize((size_t)h.esc_cap * 2);
   bool ok = fread(out->log_tab.data(), 4, out->log_tab.size(), f) == out->log_tab.size() &&
             fread(out->exp_tab.data(), 4, out->exp_tab.size(), f) == out->exp_tab.size() &&
-            fread(out->em1_bitmap.data(), 4, out->em1_bitmap.size(), f) == out->em1_bitmap.size();
+            fread(out->em1_bitmap.data(), 4, out->em1_bitmap.size(), f) == out->em1_bitmap.size() &&
+            fread(out->esc_tab.data(), 4, out->esc_tab.size(), f) == out->esc_tab.size() &&
+            fread(&out->small, sizeof out->small, 1, f) == 1;
   fclose(f);
   if (!ok) {
     snprintf(err, errlen, "truncated table file %s", path);
