@@ -337,9 +337,11 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
   {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
-    int k = sms / std::max(1, nf);
+    // speculation pays even on a full GPU (it shortens the slowest codeword of
+    // every lockstep bitplane step); at least 8 blocks per codeword, more when SMs are idle
+    int k = std::max(8, sms / std::max(1, nf));
     if (const char *e = getenv("DVC_LDPCA_SPEC")) k = atoi(e);
-    spec_k_ = std::max(1, std::min(8, k));
+    spec_k_ = std::max(1, std::min(32, k));
     if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_))) return ctx.fail("device allocation failed");
   }
   steps_ = steps;
@@ -437,28 +439,47 @@ void FrameBatcher::harvest(ProfileStats *prof) {
   ev_used_ = 0;
 }
 
-bool FrameBatcher::collect(Context &ctx, std::vector<FrameResult> &results, cudaStream_t s) {
-  const int nf = nf_;
-  results.assign(nf, FrameResult());
-  const std::vector<int> &qb = qb_;
+bool FrameBatcher::enqueue_results(Context &ctx, cudaStream_t s) {
   uint8_t *rp = (uint8_t *)pinned_ + res_off_;
   size_t ro = 0;
-  for (int f = 0; f < nf; f++) {
-    if (!ctx.cuda_ok(cudaMemcpyAsync(rp + ro, slots_[f].out.p, (size_t)qb[f] * 20, cudaMemcpyDeviceToHost, s), "D2H"))
+  for (int f = 0; f < nf_; f++) {
+    if (!ctx.cuda_ok(cudaMemcpyAsync(rp + ro, slots_[f].out.p, (size_t)qb_[f] * 20, cudaMemcpyDeviceToHost, s), "D2H"))
       return false;
-    ro += (size_t)qb[f] * 20;
+    ro += (size_t)qb_[f] * 20;
   }
-  if (!ctx.cuda_ok(cudaStreamSynchronize(s), "decode")) return false;
-  ro = 0;
-  for (int f = 0; f < nf; f++) {
+  return true;
+}
+
+void FrameBatcher::read_results(std::vector<FrameResult> &results) {
+  results.assign(nf_, FrameResult());
+  const uint8_t *rp = (const uint8_t *)pinned_ + res_off_;
+  size_t ro = 0;
+  for (int f = 0; f < nf_; f++) {
     results[f].wz_bits = wz_bits0_[f];
     const int *r = (const int *)(rp + ro);
-    const float *e = (const float *)(rp + ro + (size_t)qb[f] * 16);
-    results[f].planes.assign(r, r + qb[f] * 4);
-    results[f].entropy.assign(e, e + qb[f]);
-    for (int p = 0; p < qb[f]; p++) results[f].wz_bits += r[4 * p];
-    ro += (size_t)qb[f] * 20;
+    const float *e = (const float *)(rp + ro + (size_t)qb_[f] * 16);
+    results[f].planes.assign(r, r + qb_[f] * 4);
+    results[f].entropy.assign(e, e + qb_[f]);
+    for (int p = 0; p < qb_[f]; p++) results[f].wz_bits += r[4 * p];
+    ro += (size_t)qb_[f] * 20;
   }
+}
+
+size_t FrameBatcher::device_bytes() const {
+  size_t b = frames_dev_.bytes + jobs_dev_.bytes + spec_.bytes;
+  for (const Slot &S : slots_) {
+    const DevBuf *all[] = {&S.si, &S.dbf, &S.residue, &S.side_trans, &S.recons_trans, &S.alpha, &S.lr, &S.oct,
+                           &S.smf, &S.pdf, &S.mb_mv, &S.fmv, &S.blk_mv, &S.blk_mv2, &S.holes, &S.mse, &S.stats,
+                           &S.in, &S.out};
+    for (const DevBuf *d : all) b += d->bytes;
+  }
+  return b;
+}
+
+bool FrameBatcher::collect(Context &ctx, std::vector<FrameResult> &results, cudaStream_t s) {
+  if (!enqueue_results(ctx, s)) return false;
+  if (!ctx.cuda_ok(cudaStreamSynchronize(s), "decode")) return false;
+  read_results(results);
   return true;
 }
 

@@ -67,6 +67,12 @@ class FrameBatcher {
   bool prepare(Context &ctx, const std::vector<FrameSpec> &frames, cudaStream_t stream);
   bool execute(Context &ctx, cudaStream_t stream, int max_iter = 50, ProfileStats *prof = nullptr);
   bool collect(Context &ctx, std::vector<FrameResult> &results, cudaStream_t stream);
+  // asynchronous form of collect: enqueue the result copies on the stream, and
+  // after the stream has passed them (event or sync) parse them on the host
+  bool enqueue_results(Context &ctx, cudaStream_t stream);
+  void read_results(std::vector<FrameResult> &results);
+  // device bytes held by the batcher's slots
+  size_t device_bytes() const;
   // after the stream has been synchronised: add the recorded LDPCA event times to prof
   void harvest(ProfileStats *prof);
   bool decode(Context &ctx, const std::vector<FrameSpec> &frames, std::vector<FrameResult> &results,

@@ -49,6 +49,8 @@ def lib():
             L.dvc_LdpcaDecoder.restype = C.c_int
             L.dvc_session_destroy.argtypes = [C.c_void_p]
             L.dvc_session_destroy.restype = None
+            L.dvc_server_destroy.argtypes = [C.c_void_p]
+            L.dvc_server_destroy.restype = None
             _declare_frame_api(L)
             _lib = L
     return _lib
@@ -80,6 +82,12 @@ FRAME_API = {
     "dvc_session_run": [C.c_void_p, C.c_int, C.POINTER(C.c_double)],
     "dvc_session_frame": [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p],
     "dvc_session_profile": [C.c_void_p, C.c_void_p],
+    "dvc_server_create": [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
+    "dvc_server_submit": [C.c_void_p, C.POINTER(WZFrame), C.POINTER(C.c_longlong)],
+    "dvc_server_poll": [C.c_void_p, C.POINTER(C.c_int)],
+    "dvc_server_result": [C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(C.c_int), C.c_void_p,
+                          C.POINTER(C.c_double)],
+    "dvc_server_stats": [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_size_t)],
     "dvc_ldpca_decode_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
@@ -181,6 +189,10 @@ class Context:
             outs.append(len(crc))
         return arr, keep, outs
 
+    def server(self, mem_budget_bytes=16 << 30, streams=8, max_cohort=8):
+        """Continuous-batching server (dvc_server_*)."""
+        return Server(self, mem_budget_bytes, streams, max_cohort)
+
     def session(self, items, max_batch=0, streams=1):
         """Device-resident session over independent frames (dvc_session_*)."""
         return Session(self, items, max_batch, streams)
@@ -265,6 +277,55 @@ class Session:
     def close(self):
         if self._h:
             lib().dvc_session_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """dvc_server: submit() frames from any stream, poll() to schedule, result() to collect."""
+
+    def __init__(self, ctx, mem_budget_bytes, streams, max_cohort):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        ctx.check(lib().dvc_server_create(ctx.handle, mem_budget_bytes, streams, max_cohort, C.byref(self._h)))
+        self._meta = {}
+
+    def submit(self, item):
+        arr, keep, qbits = self.ctx._frame_array([item])
+        t = C.c_longlong(0)
+        self.ctx.check(lib().dvc_server_submit(self._h, arr, C.byref(t)))
+        self._meta[t.value] = (item["width"], item["height"], qbits[0])
+        return t.value
+
+    def poll(self):
+        n = C.c_int(0)
+        self.ctx.check(lib().dvc_server_poll(self._h, C.byref(n)))
+        return n.value
+
+    def result(self, ticket):
+        """Result of a finished ticket; raises DvcError if it has not finished."""
+        w, h, qb = self._meta[ticket]
+        rec = np.zeros((h, w), np.uint8)
+        bits = C.c_int(0)
+        planes = np.zeros((qb, 4), np.int32)
+        lat = C.c_double(0)
+        self.ctx.check(lib().dvc_server_result(self._h, ticket, _ptr(rec), C.byref(bits), _ptr(planes), C.byref(lat)))
+        del self._meta[ticket]
+        return dict(recon=rec, wz_bits=bits.value, planes=planes, latency_ms=lat.value)
+
+    def stats(self):
+        p, f, b = C.c_longlong(0), C.c_longlong(0), C.c_size_t(0)
+        self.ctx.check(lib().dvc_server_stats(self._h, C.byref(p), C.byref(f), C.byref(b)))
+        return dict(pending=p.value, in_flight=f.value, bytes_in_flight=b.value)
+
+    def close(self):
+        if self._h:
+            lib().dvc_server_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -85,7 +85,8 @@ typedef struct {
   const uint8_t *acc_synd;     /* [qbits * w*h/128] accumulated syndromes, bitstream byte layout */
   uint8_t *recon;              /* [w*h] in: intra-block pixels (if any); out: decoded frame before deblocking */
   int wz_bits;                 /* out: 10 per coded AC band + sum over bitplanes of (m+8) */
-  int *plane_results;          /* out [qbits*4] or NULL: rate, first code, accepted code, BP iterations */
+  int *plane_results;          /* out [qbits*4] or NULL: rate, first code, accepted code, and the BP
+                                  iterations run (a work counter: it grows with the speculation width) */
   float *plane_entropy;        /* out [qbits] or NULL */
   uint8_t *deblock_flag;       /* out [w*h] or NULL: coefficients changed by reconstruction */
 } dvc_wz_frame;
@@ -150,6 +151,29 @@ int dvc_session_frame(dvc_session *ses, int index, uint8_t *recon, int *wz_bits,
  * [2] LDPCA codewords, [3] kernel launches, [4] runs. */
 int dvc_session_profile(dvc_session *ses, double *out5);
 void dvc_session_destroy(dvc_session *ses);
+
+/* Continuous-batching decode server (no counterpart in the reference, which
+ * decodes one frame at a time).  Requests from any number of streams are
+ * queued by dvc_server_submit (inputs are copied, so the caller's buffers can
+ * be reused at once) and scheduled by dvc_server_poll: each of `streams` CUDA
+ * streams runs one cohort at a time, a cohort being up to `max_cohort` queued
+ * frames of one size and quantiser.  Frames are admitted while the estimated
+ * device memory of the frames in flight stays within `mem_budget_bytes`; a
+ * frame that alone exceeds the budget is refused with DVC_E_NOMEM.  Every
+ * stage, including the per-bitplane syndrome-request feedback, stays on the
+ * device; the host only submits, polls and collects.  The server must be polled
+ * from one thread at a time. */
+typedef struct dvc_server dvc_server;
+int dvc_server_create(dvc_ctx *ctx, size_t mem_budget_bytes, int streams, int max_cohort, dvc_server **out);
+int dvc_server_submit(dvc_server *srv, const dvc_wz_frame *frame, long long *ticket);
+/* Retire finished cohorts and start new ones; *completed = frames finished by this call. */
+int dvc_server_poll(dvc_server *srv, int *completed);
+/* Result of a finished request (each output may be NULL); frees the request.
+ * latency_ms: from dvc_server_submit to the poll that saw it finished. */
+int dvc_server_result(dvc_server *srv, long long ticket, uint8_t *recon, int *wz_bits, int *plane_results,
+                      double *latency_ms);
+int dvc_server_stats(dvc_server *srv, long long *pending, long long *in_flight, size_t *bytes_in_flight);
+void dvc_server_destroy(dvc_server *srv);
 
 #ifdef __cplusplus
 }

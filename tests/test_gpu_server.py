@@ -1,0 +1,57 @@
+"""GPU: the continuous-batching server gives every frame the same result as decoding
+it alone, with QCIF and CIF requests from several streams in flight together."""
+import os
+import time
+
+import numpy as np
+import pytest
+
+from dvc_b200 import bitstream as bs
+from dvc_b200 import decoder, encoder, native, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _items(kind, n_frames, gop, q, seed):
+    ori, key = synth.make_sequence(kind, n_frames, seed)
+    st = bs.parse_wz(encoder.encode_sequence(ori, gop, q))
+    return [decoder.frame_item(st, st.frames[m], key) for (m, b, e) in bs.sequence_order(st.n_frames, st.gop)]
+
+
+def test_server_mix_matches_alone(gpu_ctx):
+    mix = (_items("qcif", 5, 2, 4, 31) + _items("cif", 3, 2, 3, 32) + _items("qcif", 5, 4, 8, 33)
+           + _items("qcif", 3, 2, 1, 34) + _items("cif", 3, 2, 6, 35))
+    alone = [gpu_ctx.decode_wz_frames([it])[0] for it in mix]
+    srv = gpu_ctx.server(mem_budget_bytes=4 << 30, streams=3, max_cohort=2)
+    tickets = []
+    # staggered arrivals: half now, the rest while the first cohorts are decoding
+    for it in mix[: len(mix) // 2]:
+        tickets.append(srv.submit(it))
+    srv.poll()
+    for it in mix[len(mix) // 2:]:
+        tickets.append(srv.submit(it))
+        srv.poll()
+    done = 0
+    t0 = time.time()
+    while done < len(mix) and time.time() - t0 < 120:
+        done += srv.poll()
+        time.sleep(0.001)
+    assert done == len(mix)
+    for t, a in zip(tickets, alone):
+        r = srv.result(t)
+        assert np.array_equal(r["recon"], a["recon"])
+        assert r["wz_bits"] == a["wz_bits"]
+        # rate, first code and accepted code per bitplane; column 3 counts the BP
+        # iterations run, which depends on how widely the ladder was speculated
+        assert np.array_equal(r["planes"][:, :3], a["planes"][:, :3])
+        assert r["latency_ms"] > 0
+    srv.close()
+
+
+def test_server_refuses_frame_above_budget(gpu_ctx):
+    it = _items("cif", 3, 2, 4, 36)[0]
+    srv = gpu_ctx.server(mem_budget_bytes=1 << 20, streams=1, max_cohort=1)
+    with pytest.raises(native.DvcError) as ex:
+        srv.submit(it)
+    assert ex.value.code == native.DVC_E_NOMEM
+    srv.close()
