@@ -63,8 +63,7 @@ bool Context::init(const char *data, const char *tables, int dev) {
     *dst = (const uint32_t *)p;
     return true;
   };
-  if (!up(xlm_host.log_tab, &xlm.log_tab) || !up(xlm_host.exp_tab, &xlm.exp_tab) ||
-      !up(xlm_host.em1_bitmap, &xlm.em1_bitmap) || !up(xlm_host.esc_tab, &xlm.esc_tab))
+  if (!up(xlm_host.log_tab, &xlm.log_tab) || !up(xlm_host.exp_tab, &xlm.exp_tab))
     return fail("uploading libm tables failed");
   {
     void *p = nullptr;
@@ -83,11 +82,20 @@ bool Context::init(const char *data, const char *tables, int dev) {
   xlm.exp_mask = xlm_host.hdr.exp_cap - 1;
   xlm.log_shift = 32 - lg2(xlm_host.hdr.log_cap);
   xlm.exp_shift = 32 - lg2(xlm_host.hdr.exp_cap);
-  // no escapes: skip the escape lookup entirely
-  xlm.esc_mask = xlm_host.hdr.esc_count ? xlm_host.hdr.esc_cap - 1 : 0;
-  xlm.esc_shift = 32 - lg2(xlm_host.hdr.esc_cap);
   xlm.tanh_ylo = xlm_host.hdr.tanh_ylo;
   xlm.tanh_y1 = xlm_host.hdr.tanh_y1;
+  {
+    // phi = -logf(tanhf(y)) for every float y in [tanh_ylo, tanh_y1), from the C library
+    const size_t count = (size_t)xlm.tanh_y1 - xlm.tanh_ylo;
+    std::vector<float> phi(count);
+    dvc_phi_build(phi.data(), xlm.tanh_ylo, xlm.tanh_y1, 0);
+    void *p = nullptr;
+    if (cudaMalloc(&p, count * sizeof(float)) != cudaSuccess) return fail("phi table allocation failed");
+    xlm_allocs.push_back(p);
+    if (cudaMemcpy(p, phi.data(), count * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail("uploading the phi table failed");
+    xlm.phi_tab = (const float *)p;
+  }
 
   // LDPCA ladders (QCIF n=1584 and CIF n=6336)
   const std::string lpath = data_dir + "/ldpca_ladders.bin";

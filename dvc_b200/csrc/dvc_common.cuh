@@ -75,27 +75,15 @@ __device__ __forceinline__ float xl_expf(const XlmDev &t, const XlSmall &s, floa
   return xl_hash_lookup(t.exp_tab, t.exp_mask, t.exp_shift, u, m);
 }
 
-// tanhf as the C library computes it, for y >= 2^-31
-__device__ __forceinline__ float xl_tanhf(const XlmDev &t, const XlSmall &s, float y) {
+// -logf(tanhf(y)), the reference's two library calls (LdpcaDecoder.cpp:513,519),
+// from the direct table over [tanh_ylo, tanh_y1); -0 where tanhf(y) is 1.
+// Every argument the decoder forms is (x + 1e-9f)/2 with x >= 0, so it is at
+// least 5e-10 > 2^-31 = tanh_ylo; a smaller one (never formed) clamps to the
+// first entry rather than reading outside the table.
+__device__ __forceinline__ float xl_phi(const XlmDev &t, float y) {
   const uint32_t u = __float_as_uint(y);
-  if (u >= t.tanh_y1) return 1.0f;  // also NaN/negative patterns, which the decoder never forms
-  if (u < t.tanh_ylo) return y;     // below every argument the decoder forms; keeps the bitmap read in range
-  const bool big = y >= 1.0f;
-  const float a = big ? __fmul_rn(2.0f, y) : __fmul_rn(-2.0f, y);
-  const double d = xl_expm1_d((double)a, s);
-  float e = __double2float_rn(d);
-  const uint32_t i = u - t.tanh_ylo;
-  if ((__ldg(t.em1_bitmap + (i >> 5)) >> (i & 31)) & 1u) {
-    const float st = xl_step_toward(e, d);
-    e = t.esc_mask ? xl_hash_lookup(t.esc_tab, t.esc_mask, t.esc_shift, u, st) : st;
-  }
-  const float den = __fadd_rn(e, 2.0f);
-  return big ? __fsub_rn(1.0f, __fdiv_rn(2.0f, den)) : __fdiv_rn(-e, den);
-}
-
-// -log(tanh(y)) with the reference's two library calls (LdpcaDecoder.cpp:513,519)
-__device__ __forceinline__ float xl_phi(const XlmDev &t, const XlSmall &s, float y) {
-  return -xl_logf(t, s, xl_tanhf(t, s, y));
+  if (u >= t.tanh_y1) return -0.0f;  // also NaN/negative patterns, which the decoder never forms
+  return __ldg(t.phi_tab + (u > t.tanh_ylo ? u - t.tanh_ylo : 0u));
 }
 
 }  // namespace dvc

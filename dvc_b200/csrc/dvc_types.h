@@ -7,10 +7,10 @@ namespace dvc {
 // LDPCA ladder for one codeword length, resident in device memory.
 // Derived from the reference's ladder tables (ReadLdpcaLadderFile_LdpcaDecoder.cpp:150-201):
 // per code c the syndrome length m_c = (n/period)*bpp[c], its rate m_c/n, the
-// row of every edge ir_c[e], plus layouts this decoder adds for parallel BP:
-// per code the edges of each row in increasing edge order (row_ptr/row_edge,
-// so that row sums keep the reference's summation order), the column of every
-// edge, the CRC-8 contribution of each single source bit, and the GF(2)
+// row of every edge, plus layouts this decoder adds for parallel BP: per code
+// the row-order positions of the edges (each row's edges contiguous, in
+// increasing edge order, so that row sums keep the reference's summation
+// order), the CRC-8 contribution of each single source bit, and the GF(2)
 // inverse of the full-rate matrix with bit i of row j at word i/32, bit i%32.
 struct LadderDev {
   int n, e, period, num_codes, invh_words;
@@ -19,10 +19,12 @@ struct LadderDev {
   const int *idx;         // [num_codes*period]
   const int *synd_len;    // [num_codes]
   const float *code_rate; // [num_codes]
-  const int *row_ptr;     // [num_codes*(n+1)]
-  const uint16_t *row_edge;  // [num_codes*e]
-  const uint16_t *ir;        // [num_codes*e]
-  const uint16_t *edge_col;  // [e]
+  const int *row_ptr;     // [num_codes*(n+1)] first row-order position of each row
+  // Edges are numbered column-major (edge e = 3k + i is the i-th edge of column
+  // k, every column has degree 3); row-order position p lists each row's edges
+  // in increasing e, rows in order.
+  const uint16_t *pos;       // [num_codes*e] row-order position of edge e
+  const uint16_t *rid;       // [num_codes*e] row of row-order position p
   const uint8_t *crc_tab;    // [n]
   const uint32_t *invh;      // [n*invh_words]
 };

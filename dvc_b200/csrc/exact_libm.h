@@ -7,7 +7,7 @@
 // code, decoded bits) depend on those exact float results, so the device must
 // return the same bits as that library for every input the decoder can feed.
 //
-// Method (two parts):
+// Method:
 //  1. xl_*_d: double-precision evaluations written here from the table-driven
 //     method of P. T. P. Tang ("Table-driven implementation of the exponential
 //     function", ACM TOMS 15(2), 1989; "... of the logarithm function", ACM TOMS
@@ -15,7 +15,6 @@
 //     multiply-adds, so host and device produce identical bits:
 //       exp:   x = (32k + j) ln2/32 + r, |r| <= ln2/64; e^x = 2^k * T[j] * P(r)
 //              with T[j] = 2^(j/32) and P the degree-6 Taylor polynomial;
-//       expm1: degree-9 Taylor polynomial for |a| < 2^-5, else exp(a) - 1;
 //       log:   x = 2^e * m, m in [1, 2) split into 128 bins; per bin a
 //              reciprocal centre 1/c and log c (bins at and above sqrt 2 fold
 //              into [sqrt(1/2), 1) so that values near 1 keep full relative
@@ -27,16 +26,13 @@
 //     except in rare near-tie cases.
 //  2. Correction tables built on the host by sweeping the C library over the
 //     exact input domain (libm_tables.cpp): the inputs where the library's float
-//     result differs from part 1, with the library's value.  For expm1f a bitmap
-//     marks the exceptions; the library's value is then the float neighbour on
-//     the side of part 1's double value, except for a few inputs kept in a
-//     small escape hash.  The builder verifies this for every input.
+//     result differs from part 1, with the library's value, in a hash.
 //
-// tanhf is not swept directly: over the whole decoder domain the library's
-// tanhf(y) equals, bit for bit, 1 - 2/(expm1f(2y)+2) for y >= 1 and
-// -e/(e+2) with e = expm1f(-2y) for y < 1, evaluated in float; and it is
-// exactly 1 from a threshold y1 upward.  The builder checks this identity for
-// every y in the domain before writing any table.
+// The belief-propagation magnitude phi(y) = -logf(tanhf(y)) is not evaluated
+// at all: its argument is a float in [2^-31, y1) (y1 = the first float with
+// tanhf(y) == 1, above which phi is -0), so the library's value of the whole
+// expression is tabulated once per context for every one of those 2.9e8
+// floats (1.1 GB of device memory) and read with one load.
 #pragma once
 #include <math.h>
 #include <stdint.h>
@@ -111,22 +107,6 @@ XL_HD double xl_exp_d(double x, const XlSmall &s) {
   return ((s.exp2j[j] * er) * s1) * s2;
 }
 
-// e^a - 1 for a in [-2, 20]
-XL_HD double xl_expm1_d(double a, const XlSmall &s) {
-  if (a > -0.03125 && a < 0.03125) {
-    double q = 1.0 / 362880.0;
-    q = XL_FMA(q, a, 1.0 / 40320.0);
-    q = XL_FMA(q, a, 1.0 / 5040.0);
-    q = XL_FMA(q, a, 1.0 / 720.0);
-    q = XL_FMA(q, a, 1.0 / 120.0);
-    q = XL_FMA(q, a, 1.0 / 24.0);
-    q = XL_FMA(q, a, 1.0 / 6.0);
-    q = XL_FMA(q, a, 0.5);
-    return XL_FMA(a * a, q, a);
-  }
-  return xl_exp_d(a, s) - 1.0;
-}
-
 // natural log of a positive double that came from a float (normal as a double)
 XL_HD double xl_log_d(double x, const XlSmall &s) {
   const uint64_t u = xl_dbits(x);
@@ -149,18 +129,7 @@ XL_HD double xl_log_d(double x, const XlSmall &s) {
 
 // float results of part 1, before corrections
 XL_HD float xl_expf_base(float x, const XlSmall &s) { return XL_D2F(xl_exp_d((double)x, s)); }
-XL_HD float xl_expm1f_base(float a, const XlSmall &s) { return XL_D2F(xl_expm1_d((double)a, s)); }
 XL_HD float xl_logf_base(float x, const XlSmall &s) { return XL_D2F(xl_log_d((double)x, s)); }
-
-// the float neighbour of r on the side of the double value d (d != r)
-XL_HD float xl_step_toward(float r, double d) {
-  uint32_t u = xl_fbits(r);
-  const bool up = d > (double)r;
-  // r is finite and nonzero in every domain used here
-  if ((u >> 31) == 0) u = up ? u + 1 : u - 1;
-  else u = up ? u - 1 : u + 1;
-  return xl_bitsf(u);
-}
 
 // ---- domains (float bit patterns, inclusive) swept by the table builder ----
 // logf inputs: LLR from LR in [1e-4/0.9999, 0.9999/1e-4], tanh values in
@@ -171,5 +140,5 @@ XL_HD float xl_step_toward(float r, double d) {
 // expf inputs: -alpha*d and -0.01*SSE, always <= 0; below -104 the result is 0
 #define XL_EXP_LO 0x80000000u  // -0.0f  (negative floats ordered by magnitude)
 #define XL_EXP_HI 0xc2d00000u  // -104.0f
-// tanh arguments y = (x + 1e-9)/2 >= 5e-10; expm1f arguments -2y (y < 1) or 2y
+// tanh arguments y = (x + 1e-9)/2 with x >= 0, so y >= 5e-10
 #define XL_TANH_YLO 0x30000000u  // 2^-31, below the smallest y = 1e-9f/2 (0x3009705f)

@@ -120,7 +120,7 @@ void FrameBatcher::release() {
 
 static size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
-bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, cudaStream_t s) {
+bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, cudaStream_t s, int concurrent) {
   const int nf = (int)frames.size();
   nf_ = 0;
   if (nf == 0) return true;
@@ -339,7 +339,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
     // speculation pays even on a full GPU (it shortens the slowest codeword of
     // every lockstep bitplane step); at least 8 blocks per codeword, more when SMs are idle
-    int k = std::max(8, sms / std::max(1, nf));
+    int k = std::max(8, sms / std::max(1, std::max(nf, concurrent)));
     if (const char *e = getenv("DVC_LDPCA_SPEC")) k = atoi(e);
     spec_k_ = std::max(1, std::min(32, k));
     if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_))) return ctx.fail("device allocation failed");

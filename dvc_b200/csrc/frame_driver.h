@@ -64,7 +64,9 @@ class FrameBatcher {
   // prepare: per-frame constants, block lists, packed inputs, descriptors and
   // LDPCA jobs, uploaded once; execute: the kernels only (no host transfer, no
   // synchronisation); collect: per-bitplane results to the host.
-  bool prepare(Context &ctx, const std::vector<FrameSpec> &frames, cudaStream_t stream);
+  // concurrent_frames: frames expected to decode on the device at the same time
+  // (this batch included; 0 = this batch alone), which sets the speculation width
+  bool prepare(Context &ctx, const std::vector<FrameSpec> &frames, cudaStream_t stream, int concurrent_frames = 0);
   bool execute(Context &ctx, cudaStream_t stream, int max_iter = 50, ProfileStats *prof = nullptr);
   bool collect(Context &ctx, std::vector<FrameResult> &results, cudaStream_t stream);
   // asynchronous form of collect: enqueue the result copies on the stream, and

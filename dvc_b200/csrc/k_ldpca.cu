@@ -23,12 +23,28 @@
 //    full-rate inverse when none), so results are identical to the sequential
 //    ladder while idle SMs shorten it.
 //
-// Shared memory per codeword (n bits, e edges; CIF n=6336, e=19008), ~167 KB CIF:
-//   msg[e] f32  edge messages, in place: phi(|v->c|) -> c->v -> next phi(|v->c|)
-//   sg8[e] u8   sign of each v->c message
-//   llr[n], rowt[n] f32; dec[n], synd[n] (bit 1: row sign parity), acc[n] u8;
-//   the small exp/log tables of exact_libm.
+// Edge messages are kept in row order (each row's edges contiguous, in
+// increasing edge index), so a row sum is a sequential pass over contiguous
+// shared memory in the reference's summation order; columns (every column has
+// degree 3) reach their edges through the per-code position array.  The
+// parity check of an iteration's hard decision is folded into the next row
+// pass.  The magnitude phi(y) = -logf(tanhf(y)) is one read of the direct
+// table (dvc_common.cuh), and the reads of a pass are issued in batches so
+// that several are in flight per thread.  Shared memory is kept under 132 KB
+// so that the rest of the SM's 256 KB stays L1 cache: the per-code position
+// arrays and the table reads live there, and the L1 also bounds how many
+// table reads an SM can have in flight.
+//
+// Shared memory per codeword (n bits, e edges; CIF n=6336, e=19008: 124 KB):
+//   msg[e]  f32  edge messages by row-order position, in place:
+//                phi(|v->c|) -> c->v -> next phi(|v->c|)
+//   rowt[n] f32  row sums (after decoding: the decoded bits, one byte each)
+//   sgd[e]  u8   bit 0: sign of the v->c message, bit 1: hard decision of its column
+//   rpar[n] u8   bit 0: syndrome bit of the row, bit 1: sign parity of the row
+// The log-LRs of a thread's columns stay in registers.
 #include <cuda_runtime.h>
+
+#include <atomic>
 
 #include "dvc_common.cuh"
 #include "dvc_types.h"
@@ -39,13 +55,15 @@ namespace dvc {
 #define LDPCA_LOG2 (0.693147181f)  // LdpcaDecoder.cpp:18
 #define LDPCA_NONE 0x7f7f7f7f      // "no success yet" (memset pattern 0x7f)
 
+// largest codeword length; each thread keeps the log-LRs of up to
+// LDPCA_MAX_N / NT columns in registers
+#define LDPCA_MAX_N 6336
+
 static __host__ __device__ size_t ldpca_smem_bytes(int n, int e) {
-  size_t b = sizeof(XlmSmallTables);
-  b += (size_t)e * 4;   // msg
-  b += (size_t)n * 4;   // llr
-  b += (size_t)n * 4;   // rowt
-  b += (size_t)e;       // sg8
-  b += (size_t)n * 3;   // dec, synd, acc
+  size_t b = (size_t)e * 4;  // msg
+  b += (size_t)n * 4;        // rowt
+  b += (size_t)e;            // sgd
+  b += (size_t)n;            // rpar
   return (b + 15) & ~(size_t)15;
 }
 
@@ -94,40 +112,59 @@ __device__ __forceinline__ void build_syndrome(const LadderDev &L, int code, con
   }
 }
 
+// the same from the packed accumulated-syndrome bytes (MSB first, ByteToBit)
+__device__ __forceinline__ uint8_t acc_bit(const uint8_t *packed, int i) {
+  return (uint8_t)((__ldg(packed + (i >> 3)) >> (7 - (i & 7))) & 1);
+}
+__device__ __forceinline__ void build_syndrome_packed(const LadderDev &L, int code, const uint8_t *packed,
+                                                      uint8_t *synd) {
+  const int m = L.synd_len[code], nb = L.bpp[code];
+  const int *idx = L.idx + (size_t)code * L.period;
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    uint8_t s = acc_bit(packed, idx[k % nb] + (k / nb) * L.period);
+    if (k > 0) s ^= acc_bit(packed, idx[(k - 1) % nb] + ((k - 1) / nb) * L.period);
+    synd[k] = s;
+  }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 1)
     ldpca_ladder_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, XlmDev xt, int max_iter, int K,
                         LdpcaSpec sp) {
+  constexpr int MAXC = (LDPCA_MAX_N + NT - 1) / NT;  // columns per thread
+  constexpr int UNR = 8;                             // edge-pass table reads in flight per thread
+  constexpr int CB = NT >= 1024 ? 1 : 4;             // column-pass columns per batch (3 reads each)
   extern __shared__ __align__(16) uint8_t smem[];
   const int j = blockIdx.x / K, kk = blockIdx.x - j * K;
   const LdpcaJob J = jobs[j];
   if (!J.active) return;
   const bool spec = sp.best != nullptr;
   const int n = L.n, E = L.e, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  XlmSmallTables *tabs = reinterpret_cast<XlmSmallTables *>(smem);
-  float *msg = reinterpret_cast<float *>(smem + sizeof(XlmSmallTables));
-  float *llr = msg + E;
-  float *rowt = llr + n;
-  uint8_t *sg8 = reinterpret_cast<uint8_t *>(rowt + n);
-  uint8_t *dec = sg8 + E;
-  uint8_t *synd = dec + n;
-  uint8_t *acc = synd + n;
+  float *msg = reinterpret_cast<float *>(smem);
+  float *rowt = msg + E;
+  uint8_t *sgd = reinterpret_cast<uint8_t *>(rowt + n);
+  uint8_t *rpar = sgd + E;
+  uint8_t *dec = reinterpret_cast<uint8_t *>(rowt);  // decoded bits, once BP is over
   __shared__ uint32_t s_ured[NT / 32];
   __shared__ int s_start, s_accepted, s_stop;
-  const XlSmall xs = xl_small_stage(xt, tabs);
-  __syncthreads();
+  const XlSmall xs = xl_small_global(xt);
 
   // accumulated syndrome bits (ByteToBit, LdpcaDecoder.cpp:81-107), entropy
   // terms H_k = (P(-log P + log(1-P)) - log(1-P)) / LOG2 with P = LR/(1+LR)
   // (ComputeCE), and log LR (LdpcaDecoder.cpp:665-666)
-  for (int k = tid; k < n; k += NT) {
-    acc[k] = (uint8_t)((J.acc[k >> 3] >> (7 - (k & 7))) & 1);
-    const float lr = J.lr[k];
-    const float pco = lr / (1.0f + lr);
-    const float tmp = xl_logf(xt, xs, 1.0f - pco);
-    msg[k] = (pco * (-xl_logf(xt, xs, pco) + tmp) - tmp) / LDPCA_LOG2;
-    llr[k] = xl_logf(xt, xs, lr);
-    if (J.llr_out && kk == 0) J.llr_out[k] = llr[k];
+  float llr[MAXC];
+#pragma unroll
+  for (int c = 0; c < MAXC; c++) {
+    const int k = tid + c * NT;
+    llr[c] = 0.0f;
+    if (k < n) {
+      const float lr = J.lr[k];
+      const float pco = lr / (1.0f + lr);
+      const float tmp = xl_logf(xt, xs, 1.0f - pco);
+      msg[k] = (pco * (-xl_logf(xt, xs, pco) + tmp) - tmp) / LDPCA_LOG2;
+      llr[c] = xl_logf(xt, xs, lr);
+      if (J.llr_out && kk == 0) J.llr_out[k] = llr[c];
+    }
   }
   __syncthreads();
   if (tid == 0) {
@@ -171,108 +208,137 @@ __global__ void __launch_bounds__(NT, 1)
       if (s_stop) break;
     }
     const int m = L.synd_len[code];
-    build_syndrome(L, code, acc, synd);
+    const uint16_t *__restrict__ pos = L.pos + (size_t)code * E;
+    const uint16_t *__restrict__ rid = L.rid + (size_t)code * E;
+    build_syndrome_packed(L, code, J.acc, rpar);
+    __syncthreads();
     const int *rp = L.row_ptr + (size_t)code * (n + 1);
-    const uint16_t *re = L.row_edge + (size_t)code * E;
-    const uint16_t *ir = L.ir + (size_t)code * E;
-    // first magnitudes: phi(|LLR|) on every edge of each column
-    for (int k = tid; k < n; k += NT) {
-      const float v = llr[k];
-      const bool neg = (__float_as_uint(v) >> 31) != 0;
-      const float y = ((neg ? -v : v) + 1e-9f) / 2.0f;
-      const float ph = xl_phi(xt, xs, y);
-      for (int e = L.jc[k]; e < L.jc[k + 1]; e++) {
-        msg[e] = ph;
-        sg8[e] = neg;
+    // first magnitudes: phi(|LLR|) on the three edges of each column
+    {
+      float ph[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; c++) ph[c] = xl_phi(xt, (fabsf(llr[c]) + 1e-9f) / 2.0f);
+#pragma unroll
+      for (int c = 0; c < MAXC; c++) {
+        const int k = tid + c * NT;
+        if (k < n) {
+          const uint8_t ng = (uint8_t)(__float_as_uint(llr[c]) >> 31);
+#pragma unroll
+          for (int i = 0; i < 3; i++) {
+            const int p = __ldg(pos + 3 * k + i);
+            msg[p] = ph[c];
+            sgd[p] = ng;
+          }
+        }
       }
     }
     __syncthreads();
     bool converged = false;
     int it = 0;
-    while (it < max_iter) {
-      it++;
-      // (1) rows: sum of phi in edge order, sign parity including the syndrome
-      for (int r = tid; r < m; r += NT) {
-        float s = 0.0f;
-        uint32_t par = synd[r] & 1u;
-        const int p1 = rp[r + 1];
-        for (int p = rp[r]; p < p1; p++) {
-          const int e = re[p];
-          s += msg[e];
-          par ^= sg8[e];
-        }
-        rowt[r] = s;
-        synd[r] = (uint8_t)((synd[r] & 1u) | (par << 1));
-      }
-      __syncthreads();
-      // (2) edges: c->v = phi(row sum - own phi) with the product of the other signs
-      for (int e0 = tid; e0 < E; e0 += 2 * NT) {
-        const int e1 = e0 + NT;
-        const int r0 = __ldg(ir + e0);
-        const float y0 = (rowt[r0] - msg[e0] + 1e-9f) / 2.0f;
-        float y1 = 1.0f;
-        int r1 = 0;
-        if (e1 < E) {
-          r1 = __ldg(ir + e1);
-          y1 = (rowt[r1] - msg[e1] + 1e-9f) / 2.0f;
-        }
-        const float c0 = xl_phi(xt, xs, y0);
-        const float c1 = xl_phi(xt, xs, y1);
-        msg[e0] = c0 * ((((uint32_t)synd[r0] >> 1) ^ sg8[e0]) ? -1.0f : 1.0f);
-        if (e1 < E) msg[e1] = c1 * ((((uint32_t)synd[r1] >> 1) ^ sg8[e1]) ? -1.0f : 1.0f);
-      }
-      __syncthreads();
-      // (3) columns: total in edge order, hard decision, extrinsic messages and
-      //     their phi for the next iteration
-      for (int k = tid; k < n; k += NT) {
-        const int ea = L.jc[k], eb = L.jc[k + 1];
-        float tmp = llr[k];
-        for (int e = ea; e < eb; e++) tmp += msg[e];
-        dec[k] = (uint8_t)(__float_as_uint(tmp) >> 31);
-        if (eb - ea == 3) {
-          const float v0 = tmp - msg[ea], v1 = tmp - msg[ea + 1], v2 = tmp - msg[ea + 2];
-          const bool n0 = (__float_as_uint(v0) >> 31) != 0, n1 = (__float_as_uint(v1) >> 31) != 0,
-                     n2 = (__float_as_uint(v2) >> 31) != 0;
-          const float p0 = xl_phi(xt, xs, ((n0 ? -v0 : v0) + 1e-9f) / 2.0f);
-          const float p1 = xl_phi(xt, xs, ((n1 ? -v1 : v1) + 1e-9f) / 2.0f);
-          const float p2 = xl_phi(xt, xs, ((n2 ? -v2 : v2) + 1e-9f) / 2.0f);
-          msg[ea] = p0;
-          msg[ea + 1] = p1;
-          msg[ea + 2] = p2;
-          sg8[ea] = n0;
-          sg8[ea + 1] = n1;
-          sg8[ea + 2] = n2;
-        } else {
-          for (int e = ea; e < eb; e++) {
-            const float v = tmp - msg[e];
-            const bool ng = (__float_as_uint(v) >> 31) != 0;
-            msg[e] = xl_phi(xt, xs, ((ng ? -v : v) + 1e-9f) / 2.0f);
-            sg8[e] = ng;
-          }
-        }
-      }
-      __syncthreads();
-      // (4) parity check of every row; abandon a code above a known success
+    for (;;) {
+      // (R) rows: sum of the magnitudes in edge order and the sign parity with
+      //     the syndrome bit, for the next edge pass; from the second pass on
+      //     also the parity check of the previous hard decision
       int wrong = 0;
       for (int r = tid; r < m; r += NT) {
-        uint32_t par = synd[r] & 1u;
-        const int p1 = rp[r + 1];
-        for (int p = rp[r]; p < p1; p++) par ^= dec[__ldg(L.edge_col + re[p])];
-        wrong |= (int)par;
+        const int p0 = rp[r], p1 = rp[r + 1];
+        float s = 0.0f;
+        uint32_t x = 0;  // bit 0: xor of signs, bit 1: xor of decisions
+        for (int p = p0; p < p1; p++) {
+          s += msg[p];
+          x ^= sgd[p];
+        }
+        const uint32_t syn = rpar[r] & 1u;
+        rowt[r] = s;
+        rpar[r] = (uint8_t)(syn | (((x & 1u) ^ syn) << 1));
+        wrong |= (int)(((x >> 1) ^ syn) & 1u);
       }
       if (spec && tid == 0) s_stop = *bestp < code;
-      converged = __syncthreads_or(wrong) == 0;
-      if (converged || (spec && s_stop)) break;
+      const int any_wrong = __syncthreads_or(wrong);
+      if (it > 0 && !any_wrong) {
+        converged = true;
+        break;
+      }
+      // abandon a code above a known success
+      if (it == max_iter || (spec && s_stop)) break;
+      it++;
+      // (E) edges: c->v = phi(row sum - own magnitude) with the product of
+      //     the other signs
+      for (int p0 = tid; p0 < E; p0 += UNR * NT) {
+        float c[UNR];
+        int rr[UNR];
+#pragma unroll
+        for (int q = 0; q < UNR; q++) {
+          const int p = p0 + q * NT;
+          float y = 1.0f;
+          rr[q] = 0;
+          if (p < E) {
+            rr[q] = __ldg(rid + p);
+            y = (rowt[rr[q]] - msg[p] + 1e-9f) / 2.0f;
+          }
+          c[q] = xl_phi(xt, y);
+        }
+#pragma unroll
+        for (int q = 0; q < UNR; q++) {
+          const int p = p0 + q * NT;
+          if (p < E) msg[p] = c[q] * ((((uint32_t)rpar[rr[q]] >> 1) ^ (sgd[p] & 1u)) ? -1.0f : 1.0f);
+        }
+      }
+      __syncthreads();
+      // (C) columns: total in edge order, hard decision, extrinsic messages
+      //     and their magnitudes for the next iteration
+#pragma unroll
+      for (int c0 = 0; c0 < MAXC; c0 += CB) {
+        float ph[CB][3];
+        uint32_t sb[CB][3];
+        int pp[CB][3];
+#pragma unroll
+        for (int b = 0; b < CB; b++) {
+          const int c = c0 + b, k = tid + c * NT;
+          if (c < MAXC && k < n) {
+            float mv[3];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+              pp[b][i] = __ldg(pos + 3 * k + i);
+              mv[i] = msg[pp[b][i]];
+            }
+            float tmp = llr[c];
+            tmp += mv[0];
+            tmp += mv[1];
+            tmp += mv[2];
+            const uint32_t d = __float_as_uint(tmp) >> 31;
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+              const float v = tmp - mv[i];
+              sb[b][i] = (__float_as_uint(v) >> 31) | (d << 1);
+              ph[b][i] = xl_phi(xt, (fabsf(v) + 1e-9f) / 2.0f);
+            }
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < CB; b++) {
+          const int c = c0 + b, k = tid + c * NT;
+          if (c < MAXC && k < n)
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+              msg[pp[b][i]] = ph[b][i];
+              sgd[pp[b][i]] = (uint8_t)sb[b][i];
+            }
+        }
+      }
+      __syncthreads();
     }
     total_iters += it;
-    for (int k = tid; k < m; k += NT) synd[k] &= 1u;
-    __syncthreads();
     if (!converged) continue;
+    // hard decision of each column (bit 1 of its edges' sgd) into dec, and the
     // CRC-8 of the decoded bitplane as the xor of single-bit CRCs (the CRC is
     // linear for a fixed length with zero initial value and no final xor)
     uint32_t c = 0;
-    for (int k = tid; k < n; k += NT)
-      if (dec[k]) c ^= __ldg(L.crc_tab + k);
+    for (int k = tid; k < n; k += NT) {
+      const uint8_t d = (uint8_t)((sgd[__ldg(pos + 3 * k)] >> 1) & 1u);
+      dec[k] = d;
+      if (d) c ^= __ldg(L.crc_tab + k);
+    }
     for (int o = 16; o > 0; o >>= 1) c ^= __shfl_xor_sync(0xffffffffu, c, o);
     if (lane == 0) s_ured[warp] = c;
     __syncthreads();
@@ -306,9 +372,9 @@ __global__ void __launch_bounds__(NT, 1)
   __syncthreads();
   const int accepted = s_accepted;
   if (accepted == last) {
-    build_syndrome(L, last, acc, synd);
+    build_syndrome_packed(L, last, J.acc, rpar);
     __syncthreads();
-    invh_decode(L, synd, dec, reinterpret_cast<uint32_t *>(msg));
+    invh_decode(L, rpar, dec, reinterpret_cast<uint32_t *>(msg));
   }
   if (tid == 0) {
     J.result[0] = L.synd_len[accepted] + 8;
@@ -365,13 +431,19 @@ __global__ void __launch_bounds__(256) ldpca_finalize_kernel(LadderDev L, const 
 template <int NT>
 static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_jobs, const XlmDev &xt, int max_iter,
                              int K, const LdpcaSpec &sp, cudaStream_t stream) {
+  if (L.n > LDPCA_MAX_N) return cudaErrorInvalidValue;
   const size_t smem = ldpca_smem_bytes(L.n, L.e);
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaError_t e =
-        cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+  // the attribute is per device: set it once for each device
+  static std::atomic<uint64_t> attr_set{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(attr_set.load() & bit)) {
+    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ldpca_smem_bytes(LDPCA_MAX_N, 3 * LDPCA_MAX_N));
     if (e != cudaSuccess) return e;
-    attr_done = true;
+    attr_set.fetch_or(bit);
   }
   ldpca_ladder_kernel<NT><<<num_jobs * K, NT, smem, stream>>>(L, jobs, xt, max_iter, K, sp);
   return cudaGetLastError();

@@ -106,9 +106,28 @@ bool load_ladders(const std::string &path, std::vector<LadderHost> &out, std::st
         L.row_edge[(size_t)c * L.e + fill[r]++] = (uint16_t)e;
       }
     }
-    L.edge_col.resize(L.e);
-    for (int k = 0; k < L.n; k++)
-      for (int e = L.jc[k]; e < L.jc[k + 1]; e++) L.edge_col[e] = (uint16_t)k;
+    // the decoder kernel takes every column to have degree 3 (edge e = 3k + i)
+    // and stages the per-code index arrays with 16-byte copies
+    for (int k = 0; k <= L.n; k++)
+      if (L.jc[k] != 3 * k) {
+        fclose(f);
+        err = "ladder with a column degree other than 3";
+        return false;
+      }
+    if (L.e % 8 != 0 || L.e > 65535) {
+      fclose(f);
+      err = "ladder edge count not a multiple of 8 or above 65535";
+      return false;
+    }
+    // row-order positions: pos[e] and the row of each position
+    L.pos.resize((size_t)L.num_codes * L.e);
+    L.rid.resize((size_t)L.num_codes * L.e);
+    for (int c = 0; c < L.num_codes; c++)
+      for (int p = 0; p < L.e; p++) {
+        const int e = L.row_edge[(size_t)c * L.e + p];
+        L.pos[(size_t)c * L.e + e] = (uint16_t)p;
+        L.rid[(size_t)c * L.e + p] = L.ir[(size_t)c * L.e + e];
+      }
     // CRC-8 is linear over GF(2) for a fixed message length (zero initial
     // value, no final xor), so the CRC of a bitplane is the xor of the CRCs
     // of its single set bits.
@@ -225,8 +244,8 @@ bool LadderGpu::upload(const LadderHost &L, std::string &err) {
   dev.invh_words = L.invh_words;
   return put(allocs, L.jc, &dev.jc, err) && put(allocs, L.bpp, &dev.bpp, err) && put(allocs, L.idx, &dev.idx, err) &&
          put(allocs, L.synd_len, &dev.synd_len, err) && put(allocs, L.code_rate, &dev.code_rate, err) &&
-         put(allocs, L.row_ptr, &dev.row_ptr, err) && put(allocs, L.row_edge, &dev.row_edge, err) &&
-         put(allocs, L.ir, &dev.ir, err) && put(allocs, L.edge_col, &dev.edge_col, err) &&
+         put(allocs, L.row_ptr, &dev.row_ptr, err) && put(allocs, L.pos, &dev.pos, err) &&
+         put(allocs, L.rid, &dev.rid, err) &&
          put(allocs, L.crc_tab, &dev.crc_tab, err) && put(allocs, L.invh, &dev.invh, err);
 }
 

@@ -14,7 +14,7 @@ struct LadderHost {
   int n = 0, e = 0, period = 0, num_codes = 0, invh_words = 0;
   std::vector<int> jc, bpp, idx, synd_len, row_ptr;
   std::vector<float> code_rate;
-  std::vector<uint16_t> ir, row_edge, edge_col;
+  std::vector<uint16_t> ir, row_edge, pos, rid;
   std::vector<uint8_t> crc_tab;
   std::vector<uint32_t> invh;
   std::vector<int> ir_full;  // full-rate rows (the encoder's parity-check matrix)

@@ -1,16 +1,15 @@
-// Host-side builder and loader of the correction tables that make the device
-// float functions in exact_libm.h return the C library's bits (see that
-// header for the method).  The tables are derived from the C library that the
-// reference decoder links on this host, by calling it over each input domain:
+// Host-side builder and loader of the tables that make the device float
+// functions in exact_libm.h return the C library's bits (see that header for
+// the method).  The tables are derived from the C library that the reference
+// decoder links on this host, by calling it over each input domain:
 //
 //   logf   every positive float up to 10001: hash of (input, result) pairs
 //          where the library differs from xl_logf_base;
 //   expf   every float in [-104, -0]: hash of the differing pairs;
-//   expm1f arguments +-2y of every tanh argument y in [2^-31, y1): a bitmap over
-//          y marking where the library's expm1f differs from xl_expm1f_base
-//          (the library's value is then the neighbour toward the double value);
-//   tanhf  y1 = first float with tanhf(y) == 1; the builder checks that below
-//          y1 tanhf equals the expm1f formula bit for bit.
+//   tanhf  y1 = first float with tanhf(y) == 1 (checked to stay 1 above it);
+//   phi    -logf(tanhf(y)) for every y in [2^-31, y1), the belief-propagation
+//          magnitude, as one direct table (dvc_phi_build; not stored in the
+//          file, rebuilt in about a second when a context starts).
 //
 // The file starts with the C library's version string; a loader that finds a
 // different version (or no file) rebuilds the tables.
@@ -91,11 +90,6 @@ void build_hash(const std::vector<Pair> &pairs, std::vector<uint32_t> &table, ui
   }
 }
 
-float tanh_formula(float y, float e) {
-  // glibc-equivalent evaluation order, float arithmetic
-  if (y >= 1.0f) return 1.0f - 2.0f / (e + 2.0f);
-  return -e / (e + 2.0f);
-}
 
 }  // namespace
 
@@ -145,53 +139,16 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
       return -2;
     }
 
-  // ---- expm1f bitmap over y in [ylo, y1) and the tanh identity check
-  const uint32_t ylo = XL_TANH_YLO;
-  const uint64_t ny = (uint64_t)y1 - ylo;
-  std::vector<uint32_t> bitmap((ny + 31) / 32, 0u);
-  std::atomic<long long> bad_identity(0), em1_count(0);
-  std::atomic<uint32_t> first_bad(0);
-  std::vector<std::vector<Pair>> esc_parts(threads);
-  // threads write disjoint 32-aligned word ranges
-  const uint64_t words = bitmap.size();
-  parallel_ranges(0, words - 1, threads, [&](int tid, uint64_t wa, uint64_t wb) {
-    long long cnt = 0;
-    for (uint64_t wi = wa; wi <= wb; wi++) {
-      uint32_t word = 0;
-      for (int bit = 0; bit < 32; bit++) {
-        const uint64_t i = wi * 32 + bit;
-        if (i >= ny) break;
-        const float y = xl_bitsf((uint32_t)(ylo + i));
-        const float a = (y >= 1.0f) ? 2.0f * y : -2.0f * y;
-        const float g = expm1f(a);
-        const float m = xl_expm1f_base(a, sv);
-        if (xl_fbits(g) != xl_fbits(m)) {
-          if (xl_fbits(xl_step_toward(m, xl_expm1_d((double)a, sv))) != xl_fbits(g))
-            esc_parts[tid].push_back({ylo + (uint32_t)i, xl_fbits(g)});
-          word |= 1u << bit;
-          cnt++;
-        }
-        if (xl_fbits(tanhf(y)) != xl_fbits(tanh_formula(y, g))) {
-          bad_identity++;
-          first_bad = ylo + (uint32_t)i;
-        }
-      }
-      bitmap[wi] = word;
-    }
-    em1_count += cnt;
-  });
-  if (bad_identity.load()) {
-    snprintf(err, errlen, "tanh identity failures %lld (first y bits %08x)", bad_identity.load(), first_bad.load());
-    return -3;
+  // below y1 the phi table covers [2^-31, y1); -logf(1) must be -0 above it
+  if (xl_fbits(-logf(1.0f)) != 0x80000000u) {
+    snprintf(err, errlen, "-logf(1) is not -0");
+    return -2;
   }
-  std::vector<Pair> escp;
-  for (auto &v : esc_parts) escp.insert(escp.end(), v.begin(), v.end());
 
-  std::vector<uint32_t> log_tab, exp_tab, esc_tab;
-  uint32_t log_cap = 0, exp_cap = 0, esc_cap = 0;
+  std::vector<uint32_t> log_tab, exp_tab;
+  uint32_t log_cap = 0, exp_cap = 0;
   build_hash(logp, log_tab, log_cap);
   build_hash(expp, exp_tab, exp_cap);
-  build_hash(escp, esc_tab, esc_cap);
 
   XlmHeader h;
   memset(&h, 0, sizeof h);
@@ -201,12 +158,8 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
   h.log_count = (uint32_t)logp.size();
   h.exp_cap = exp_cap;
   h.exp_count = (uint32_t)expp.size();
-  h.tanh_ylo = ylo;
+  h.tanh_ylo = XL_TANH_YLO;
   h.tanh_y1 = y1;
-  h.em1_words = (uint32_t)bitmap.size();
-  h.em1_count = (uint32_t)em1_count.load();
-  h.esc_cap = esc_cap;
-  h.esc_count = (uint32_t)escp.size();
   std::string tmp = std::string(path) + ".tmp";
   FILE *f = fopen(tmp.c_str(), "wb");
   if (!f) {
@@ -216,8 +169,6 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
   fwrite(&h, sizeof h, 1, f);
   fwrite(log_tab.data(), 4, log_tab.size(), f);
   fwrite(exp_tab.data(), 4, exp_tab.size(), f);
-  fwrite(bitmap.data(), 4, bitmap.size(), f);
-  fwrite(esc_tab.data(), 4, esc_tab.size(), f);
   fwrite(&small, sizeof small, 1, f);
   fclose(f);
   if (rename(tmp.c_str(), path) != 0) {
@@ -247,12 +198,8 @@ int dvc_libm_load(const char *path, XlmHost *out, char *err, int errlen) {
   out->hdr = h;
   out->log_tab.resize((size_t)h.log_cap * 2);
   out->exp_tab.resize((size_t)h.exp_cap * 2);
-  out->em1_bitmap.resize(h.em1_words);
-  out->esc_tab.resize((size_t)h.esc_cap * 2);
   bool ok = fread(out->log_tab.data(), 4, out->log_tab.size(), f) == out->log_tab.size() &&
             fread(out->exp_tab.data(), 4, out->exp_tab.size(), f) == out->exp_tab.size() &&
-            fread(out->em1_bitmap.data(), 4, out->em1_bitmap.size(), f) == out->em1_bitmap.size() &&
-            fread(out->esc_tab.data(), 4, out->esc_tab.size(), f) == out->esc_tab.size() &&
             fread(&out->small, sizeof out->small, 1, f) == 1;
   fclose(f);
   if (!ok) {
@@ -260,4 +207,11 @@ int dvc_libm_load(const char *path, XlmHost *out, char *err, int errlen) {
     return -2;
   }
   return 0;
+}
+
+void dvc_phi_build(float *out, uint32_t ylo, uint32_t y1, int threads) {
+  if (threads <= 0) threads = hw_threads();
+  parallel_ranges(ylo, (uint64_t)y1 - 1, threads, [&](int, uint64_t a, uint64_t b) {
+    for (uint64_t u = a; u <= b; u++) out[u - ylo] = -logf(tanhf(xl_bitsf((uint32_t)u)));
+  });
 }

@@ -3,9 +3,12 @@
 // Requests (one WZ frame each, with their reference frames) are queued by
 // submit().  poll() does the scheduling: it retires finished cohorts (an event
 // per stream tells when the device is done with one) and forms new cohorts for
-// idle streams from the queue: frames of one size and quantiser, up to
+// idle streams from the queue: frames of one size (any quantisers), up to
 // max_cohort of them, admitted while the estimated device memory of the frames
-// in flight stays within the budget.  Each cohort runs the whole frame pipeline
+// in flight stays within the budget.  While other cohorts are decoding, a
+// cohort that would start short of max_cohort waits up to the batch window for
+// company; the speculation width of its ladders is set from all frames then in
+// flight, so that many small cohorts do not oversubscribe the SMs.  Each cohort runs the whole frame pipeline
 // on its own stream (side information, noise model, every bitplane's ladder with
 // the syndrome-request feedback on the device, reconstruction, refinement), so
 // cohorts on different streams overlap on the GPU and a request that arrives
@@ -93,6 +96,8 @@ struct dvc_server {
   std::map<long long, std::shared_ptr<Request>> finished;
   long long next_ticket = 1;
   long long completed = 0;
+  // a partial cohort waits this long for company while another cohort is decoding
+  int batch_window_us = 2000;
 };
 
 static int srv_fail(dvc_server *S, int code, const std::string &m) {
@@ -172,14 +177,29 @@ static bool start_cohort(dvc_server *S, int i) {
   dvc::Context &c = *S->c;
   Cohort &C = S->cohorts[i];
   C.reqs.clear();
-  // frames of one size and quantiser, oldest first, within the memory budget
+  // frames of one size, oldest first, within the memory budget (quantisers may
+  // differ: each frame takes part only in the band/bitplane steps it codes)
   std::shared_ptr<Request> head;
+  {
+    // dynamic batching: while other cohorts keep the GPU busy, a partial cohort
+    // waits up to the batch window for more frames of its kind
+    bool busy = false;
+    for (auto &o : S->cohorts) busy = busy || o.active;
+    if (busy && !S->pending.empty()) {
+      const Request &h0 = *S->pending.front();
+      int same = 0;
+      for (auto &p : S->pending)
+        if (p->w == h0.w && p->h == h0.h) same++;
+      const double waited = std::chrono::duration<double, std::micro>(Clock::now() - h0.t_submit).count();
+      if (same < S->max_cohort && waited < S->batch_window_us) return true;
+    }
+  }
   for (auto it = S->pending.begin(); it != S->pending.end();) {
     Request &r = **it;
     if (!head) {
       if (S->used + r.est_bytes > S->budget) break;  // the oldest waits for memory
       head = *it;
-    } else if (r.w != head->w || r.h != head->h || r.q != head->q || S->used + r.est_bytes > S->budget) {
+    } else if (r.w != head->w || r.h != head->h || S->used + r.est_bytes > S->budget) {
       ++it;
       continue;
     }
@@ -241,7 +261,9 @@ static bool start_cohort(dvc_server *S, int i) {
     sp.acc = r.acc.data();
     sp.recon = C.out[f].as<uint8_t>();
   }
-  if (!C.batcher.prepare(c, specs, s) || !C.batcher.execute(c, s, 50, nullptr)) return false;
+  int in_flight = 0;
+  for (auto &o : S->cohorts) in_flight += (int)o.reqs.size();
+  if (!C.batcher.prepare(c, specs, s, in_flight) || !C.batcher.execute(c, s, 50, nullptr)) return false;
   for (int f = 0; f < nf; f++)
     if (!c.cuda_ok(cudaMemcpyAsync(C.pinned_out + f * fs, C.out[f].p, fs, cudaMemcpyDeviceToHost, s), "D2H recon"))
       return false;
@@ -311,6 +333,13 @@ extern "C" int dvc_server_stats(dvc_server *S, long long *pending, long long *in
   if (pending) *pending = (long long)S->pending.size();
   if (in_flight) *in_flight = inflight;
   if (bytes_in_flight) *bytes_in_flight = S->used;
+  return DVC_OK;
+}
+
+extern "C" int dvc_server_config(dvc_server *S, int batch_window_us) {
+  if (!S || batch_window_us < 0) return DVC_E_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->batch_window_us = batch_window_us;
   return DVC_OK;
 }
 

@@ -11,7 +11,7 @@ import threading
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libdvc_b200.so")
+LIB_PATH = os.environ.get("DVC_B200_LIB") or os.path.join(HERE, "_lib", "libdvc_b200.so")
 DATA_DIR = os.path.join(HERE, "ladders")
 TABLE_DIR = os.environ.get("DVC_B200_TABLES", os.path.join(HERE, "_tables"))
 
@@ -87,6 +87,7 @@ FRAME_API = {
     "dvc_server_poll": [C.c_void_p, C.POINTER(C.c_int)],
     "dvc_server_result": [C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(C.c_int), C.c_void_p,
                           C.POINTER(C.c_double)],
+    "dvc_server_config": [C.c_void_p, C.c_int],
     "dvc_server_stats": [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_size_t)],
     "dvc_ldpca_decode_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
@@ -189,9 +190,12 @@ class Context:
             outs.append(len(crc))
         return arr, keep, outs
 
-    def server(self, mem_budget_bytes=16 << 30, streams=8, max_cohort=8):
+    def server(self, mem_budget_bytes=16 << 30, streams=8, max_cohort=8, batch_window_us=None):
         """Continuous-batching server (dvc_server_*)."""
-        return Server(self, mem_budget_bytes, streams, max_cohort)
+        srv = Server(self, mem_budget_bytes, streams, max_cohort)
+        if batch_window_us is not None:
+            self.check(lib().dvc_server_config(srv._h, batch_window_us))
+        return srv
 
     def session(self, items, max_batch=0, streams=1):
         """Device-resident session over independent frames (dvc_session_*)."""

@@ -157,7 +157,7 @@ void dvc_session_destroy(dvc_session *ses);
  * queued by dvc_server_submit (inputs are copied, so the caller's buffers can
  * be reused at once) and scheduled by dvc_server_poll: each of `streams` CUDA
  * streams runs one cohort at a time, a cohort being up to `max_cohort` queued
- * frames of one size and quantiser.  Frames are admitted while the estimated
+ * frames of one size (quantisers may differ).  Frames are admitted while the estimated
  * device memory of the frames in flight stays within `mem_budget_bytes`; a
  * frame that alone exceeds the budget is refused with DVC_E_NOMEM.  Every
  * stage, including the per-bitplane syndrome-request feedback, stays on the
@@ -173,6 +173,9 @@ int dvc_server_poll(dvc_server *srv, int *completed);
 int dvc_server_result(dvc_server *srv, long long ticket, uint8_t *recon, int *wz_bits, int *plane_results,
                       double *latency_ms);
 int dvc_server_stats(dvc_server *srv, long long *pending, long long *in_flight, size_t *bytes_in_flight);
+/* Dynamic batching window: while another cohort is decoding, a cohort with
+ * fewer than max_cohort frames waits up to this long for more (default 2000 us). */
+int dvc_server_config(dvc_server *srv, int batch_window_us);
 void dvc_server_destroy(dvc_server *srv);
 
 #ifdef __cplusplus
