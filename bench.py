@@ -2,22 +2,27 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (one step): every WZ frame of a synthetic CIF 352x288 sequence
-(17 frames, GOP 2, the seeded generator of dvc_b200.synth "cif": six sinusoids
-with periods 8-80 px, global motion, four moving 48x48 objects, key frames =
-original + N(0,2)) encoded at each QIndex 1..8 (SkipBlock 0, IntraMode 0,
-DeblockingFilter 0) -> 64 independent WZ frames of mixed Q per step.
+Workload (one step): every WZ frame of 16 synthetic CIF 352x288 sequences, 65
+frames each: GOP 2 and GOP 4, each at QIndex 1..8 (SkipBlock 0, IntraMode 0,
+DeblockingFilter 0), the seeded generator of dvc_b200.synth "cif" (six
+sinusoids with periods 8-80 px, global motion, four moving 48x48 objects, key
+frames = original + N(0,2)) -> 8*32 + 8*48 = 640 WZ frames per step.  GOP-4
+frames 1 and 3 of each GOP take the decoded frame 2 as a reference, so a step
+has two levels of dependent frames.
 
 Our arm prints one JSON line with:
   value   WZ frames/s of the batched device-resident path (dvc_session: inputs
-          already in HBM, cohorts of 8 frames on 8 streams; device time from CUDA
-          events; L2 flushed between steps);
+          already in HBM, cohorts of frames on concurrent streams, the GOP-4
+          levels chained on the device; device time from CUDA events; L2
+          flushed between steps);
   e2e     the same through the public serving API with host buffers
-          (dvc_server: every frame of a step submitted at once, reference frames,
-          syndromes and CRCs copied in and decoded frames copied out inside the
-          timed region);
-  served  Poisson arrivals at 70% of the measured capacity through dvc_server:
-          throughput and per-frame latency p50/p99 (submit to completion);
+          (dvc_server: the frames of each level submitted at once, reference
+          frames, syndromes and CRCs copied in and decoded frames copied out
+          inside the timed region; the second level's references are the first
+          level's results);
+  served  Poisson arrivals at fractions of the measured capacity through
+          dvc_server (requests drawn from the first-level frames): throughput
+          and per-frame latency p50/p99 (submit to completion);
   plain   the one-frame-at-a-time drop-in (one dvc_decode_wz_frames call per
           frame) with per-frame latency p50/p99;
   roofline, cpu_baseline, clocks, gpu_launches.
@@ -41,25 +46,38 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "WZ frames/s + p50/p99 frame latency at CIF, served vs plain GPU, bit-exact"
-N_FRAMES, GOP, SEED, KIND = 17, 2, 101, "cif"
+N_FRAMES, SEED, KIND = 65, 101, "cif"
+GOPS = (2, 4)
 QS = tuple(range(1, 9))
 
 
 def workload():
+    """Original and key frames, and the parsed WZ stream of every (GOP, Q)."""
     from dvc_b200 import bitstream as bs, encoder, synth
     ori, key = synth.make_sequence(KIND, N_FRAMES, SEED)
-    streams = {q: bs.parse_wz(encoder.encode_sequence(ori, GOP, q)) for q in QS}
+    streams = {(g, q): bs.parse_wz(encoder.encode_sequence(ori, g, q)) for g in GOPS for q in QS}
     return ori, key, streams
 
 
 def items(streams, key):
-    from dvc_b200 import bitstream as bs, decoder
-    out = []
-    for q in QS:
-        st = streams[q]
-        for (m, b, e) in bs.sequence_order(st.n_frames, st.gop):
-            out.append(decoder.frame_item(st, st.frames[m], key))
-    return out
+    """Every WZ frame of every stream in decode order, as session items: a
+    reference that is itself a WZ frame is named by the index of its item
+    (past_from / future_from); the level of each item is returned beside it."""
+    from dvc_b200 import decoder
+    out, level = [], []
+    for (g, q), st in sorted(streams.items()):
+        where = {}
+        for lv, lvl in enumerate(decoder.decode_levels(st)):
+            for (m, b, e) in lvl:
+                it = decoder.frame_item(st, st.frames[m], key)
+                for name, ref in (("past", b), ("future", e)):
+                    if ref in st.frames:
+                        it[name + "_from"] = where[ref]
+                        it[name] = None
+                where[m] = len(out)
+                out.append(it)
+                level.append(lv)
+    return out, level
 
 
 class Clocks:
@@ -110,7 +128,6 @@ def ref_cpu_sample(ori, key, streams, q, cores, workdir):
     from oracle import refrun
     from dvc_b200 import synth, bitstream as bs
     import struct
-    st = streams[q]
     d = tempfile.mkdtemp(dir=workdir)
     oy, ky, sf = os.path.join(d, "o.yuv"), os.path.join(d, "k.yuv"), os.path.join(d, "s.txt")
     synth.write_yuv420(oy, ori[:3])
@@ -118,7 +135,7 @@ def ref_cpu_sample(ori, key, streams, q, cores, workdir):
     synth.write_frame_stat(sf, 3)
     from dvc_b200 import encoder
     wz = os.path.join(d, "s.wz")
-    open(wz, "wb").write(encoder.encode_sequence(ori[:3], GOP, q))
+    open(wz, "wb").write(encoder.encode_sequence(ori[:3], 2, q))
     intra = os.path.join(d, "s.intra")
     open(intra, "wb").close()
     t0 = time.time()
@@ -166,8 +183,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--max-batch", type=int, default=8)
-    ap.add_argument("--streams", type=int, default=8)
+    ap.add_argument("--max-batch", type=int, default=16)
+    ap.add_argument("--streams", type=int, default=16)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -184,7 +201,7 @@ def main():
     from dvc_b200 import native
 
     ori, key, streams = workload()
-    its = items(streams, key)
+    its, lev = items(streams, key)
     ctx = native.Context(local)
     ses = ctx.session(its, max_batch=args.max_batch, streams=args.streams)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
@@ -227,17 +244,34 @@ def main():
     d2h = len(its) * fs + qb * 20
     srv = ctx.server(mem_budget_bytes=16 << 30, streams=args.streams, max_cohort=args.max_batch)
 
-    def serve_all(arrivals=None):
-        """Submit its (at the given offsets in seconds, or all at once), poll to completion."""
-        order = list(range(len(its))) if arrivals is None else list(range(len(arrivals)))
+    level0 = [i for i in range(len(its)) if lev[i] == 0]
+
+    def serve_all(pool=None, arrivals=None):
+        """Submit the items of `pool` at the given offsets in seconds (pool None:
+        every item, each as soon as the items it references are done) and poll
+        to completion.  Returns (seconds, latencies in ms, results by item)."""
+        n_req = len(its) if pool is None else len(arrivals)
         tickets, lat, res = {}, [], {}
+        waiting = list(range(n_req))
         t0 = time.perf_counter()
-        nxt, done = 0, 0
-        while done < len(order):
+        done = 0
+        while done < n_req:
             now = time.perf_counter() - t0
-            while nxt < len(order) and (arrivals is None or arrivals[nxt] <= now):
-                tickets[srv.submit(its[order[nxt] % len(its)])] = nxt
-                nxt += 1
+            still = []
+            for k in waiting:
+                i = k if pool is None else pool[k % len(pool)]
+                it = its[i]
+                deps = [it.get("past_from"), it.get("future_from")]
+                if (arrivals is not None and arrivals[k] > now) or any(d is not None and d not in res for d in deps):
+                    still.append(k)
+                    continue
+                if deps[0] is not None or deps[1] is not None:
+                    it = dict(it)
+                    for name, d in zip(("past", "future"), deps):
+                        if d is not None:
+                            it[name] = res[d]["recon"]
+                tickets[srv.submit(it)] = i
+            waiting = still
             if srv.poll():
                 for t in list(tickets):
                     try:
@@ -245,8 +279,7 @@ def main():
                     except native.DvcError:
                         continue
                     lat.append(r["latency_ms"])
-                    if arrivals is None:
-                        res[tickets[t]] = r
+                    res[tickets[t]] = r
                     tickets.pop(t)
                     done += 1
             else:
@@ -267,8 +300,8 @@ def main():
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    # the served results equal the session's (both bit-exact paths)
-    for i in (0, len(its) // 2, len(its) - 1):
+    # the served results equal the session's (both bit-exact paths), second level included
+    for i in (0, len(its) // 2, len(its) - 1, max(i for i in range(len(its)) if lev[i] > 0)):
         rec_i, bits_i, _ = ses.frame(i)
         assert np.array_equal(served[i]["recon"], rec_i) and served[i]["wz_bits"] == bits_i
 
@@ -280,16 +313,16 @@ def main():
         rng = np.random.default_rng(7)
         n_req = max(64, int(rate * 2.0))
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
-        srv_dt, srv_lat, _ = serve_all(arrivals)
+        srv_dt, srv_lat, _ = serve_all(level0, arrivals)
         served_sweep.append({"offered_rate": rate, "throughput": n_req / srv_dt, "requests": n_req,
                              "p50_ms": float(np.percentile(srv_lat, 50)), "p99_ms": float(np.percentile(srv_lat, 99))})
     srv.close()
     served_main = served_sweep[2]
 
-    # plain one-frame-at-a-time drop-in: one frame per Q
+    # plain one-frame-at-a-time drop-in: one first-level frame per Q
     plain_lat = []
-    for q_i in range(len(QS)):
-        it = its[q_i * (len(its) // len(QS))]
+    for q in QS:
+        it = its[min(i for i in level0 if its[i]["qindex"] == q)]
         ctx.decode_wz_frames([it])
         t0 = time.perf_counter()
         ctx.decode_wz_frames([it])
@@ -333,8 +366,9 @@ def main():
             "metric": METRIC, "value": value, "unit": "WZ frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32/f64 (reference arithmetic, bit-exact)", "data": "synthetic",
-            "config": {"workload": "CIF 352x288, GOP 2, 17-frame sequence at QIndex 1..8 -> %d WZ frames per step "
-                                   "(SkipBlock 0, IntraMode 0, Deblock 0)" % frames_per_step,
+            "config": {"workload": "CIF 352x288, 65-frame sequences at GOP 2 and GOP 4, QIndex 1..8 -> %d WZ "
+                                   "frames per step in two dependent levels (SkipBlock 0, IntraMode 0, Deblock 0)"
+                                   % frames_per_step,
                        "frames_per_step": frames_per_step, "max_batch": args.max_batch, "streams": args.streams,
                        "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -343,7 +377,8 @@ def main():
             "plain": {"value": plain_fps, "unit": "WZ frames/s",
                       "p50_ms": 1e3 * float(np.percentile(plain_lat, 50)),
                       "p99_ms": 1e3 * float(np.percentile(plain_lat, 99)), "frames": len(plain_lat)},
-            "served": dict(served_main, unit="WZ frames/s", arrivals="Poisson at 70% of the batched capacity",
+            "served": dict(served_main, unit="WZ frames/s",
+                           arrivals="Poisson at 70% of the batched capacity, first-level frames",
                            streams=args.streams, max_cohort=args.max_batch, sweep=served_sweep),
             "roofline": {"bound": "hbm", "kernel": "ldpca_ladder_kernel", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,

@@ -6,6 +6,8 @@
 #include <new>
 #include <vector>
 
+#include <algorithm>
+#include <array>
 #include <map>
 
 #include "context.h"
@@ -288,10 +290,15 @@ static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t 
 struct dvc_session {
   dvc_ctx *ctx = nullptr;
   int w = 0, h = 0, count = 0;
-  std::vector<dvc::DevBuf> ref, lp, ip, out;
-  std::vector<std::vector<uint8_t>> host_inputs;  // copies of mode/crc/acc for prepare
+  std::vector<dvc::DevBuf> ref, lp, ip;   // reference frames given by the caller (+ derived planes)
+  std::vector<dvc::DevBuf> out, olp, oip; // decoded frames (+ derived planes of those used as references)
+  std::vector<dvc::DevBuf> init;          // initial recon (intra pixels) of frames with intra blocks
+  std::vector<char> is_ref;               // frame i's output is a reference of a later level
   std::vector<dvc::FrameBatcher> batches;
-  std::vector<std::vector<int>> batch_frames;     // frame indices of each batch
+  std::vector<std::vector<int>> batch_frames;  // frame indices of each batch
+  std::vector<std::vector<int>> batch_deps;    // batches whose outputs each batch reads
+  std::vector<int> batch_stream;
+  std::vector<cudaEvent_t> batch_done;
   std::vector<cudaStream_t> streams;
   std::vector<std::vector<dvc::FrameResult>> results;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -302,10 +309,11 @@ struct dvc_session {
 
 static void session_release(dvc_session *S) {
   for (auto &b : S->batches) b.release();
-  for (auto *v : {&S->ref, &S->lp, &S->ip, &S->out})
+  for (auto *v : {&S->ref, &S->lp, &S->ip, &S->out, &S->olp, &S->oip, &S->init})
     for (auto &b : *v) b.release();
   for (cudaStream_t st : S->streams) cudaStreamDestroy(st);
   for (cudaEvent_t e : S->done) cudaEventDestroy(e);
+  for (cudaEvent_t e : S->batch_done) cudaEventDestroy(e);
   if (S->t0) cudaEventDestroy(S->t0);
   if (S->t1) cudaEventDestroy(S->t1);
 }
@@ -326,6 +334,46 @@ extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *f
       return DVC_E_ARG;
     }
   }
+  // A reference pointer equal to another frame's recon pointer names that
+  // frame's decoded output: the frame then decodes in a later level.
+  std::map<const uint8_t *, int> recon_of;
+  for (int i = 0; i < count; i++) recon_of[frames[i].recon] = i;
+  std::vector<std::array<int, 2>> dep(count, {-1, -1});
+  std::map<const uint8_t *, int> refs;
+  for (int i = 0; i < count; i++)
+    for (int k = 0; k < 2; k++) {
+      const uint8_t *p = k == 0 ? frames[i].past : frames[i].future;
+      auto it = recon_of.find(p);
+      if (it != recon_of.end()) {
+        if (it->second == i) {
+          c.err = "dvc_session_create: frame " + std::to_string(i) + " references its own output";
+          return DVC_E_ARG;
+        }
+        dep[i][k] = it->second;
+      } else if (!refs.count(p)) {
+        const int n = (int)refs.size();
+        refs[p] = n;
+      }
+    }
+  std::vector<int> level(count, -1);
+  for (int pass = 0, left = count; left > 0; pass++) {
+    int placed = 0;
+    for (int i = 0; i < count; i++) {
+      if (level[i] >= 0) continue;
+      bool ready = true;  // every reference decoded in an earlier level
+      for (int k = 0; k < 2; k++)
+        if (dep[i][k] >= 0 && (level[dep[i][k]] < 0 || level[dep[i][k]] >= pass)) ready = false;
+      if (ready) {
+        level[i] = pass;
+        placed++;
+      }
+    }
+    if (!placed) {
+      c.err = "dvc_session_create: circular references between frames";
+      return DVC_E_ARG;
+    }
+    left -= placed;
+  }
   dvc_session *S = new (std::nothrow) dvc_session();
   if (!S) return DVC_E_NOMEM;
   S->ctx = ctx;
@@ -339,17 +387,17 @@ extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *f
     delete S;
     return code;
   };
-  std::map<const uint8_t *, int> refs;
-  for (int i = 0; i < count; i++)
-    for (const uint8_t *p : {frames[i].past, frames[i].future})
-      if (!refs.count(p)) {
-        const int k = (int)refs.size();
-        refs[p] = k;
-      }
   S->ref.resize(refs.size());
   S->lp.resize(refs.size());
   S->ip.resize(refs.size());
   S->out.resize(count);
+  S->olp.resize(count);
+  S->oip.resize(count);
+  S->init.resize(count);
+  S->is_ref.assign(count, 0);
+  for (int i = 0; i < count; i++)
+    for (int k = 0; k < 2; k++)
+      if (dep[i][k] >= 0) S->is_ref[dep[i][k]] = 1;
   cudaStream_t s0 = c.stream;
   for (auto &kv : refs) {
     const int k = kv.second;
@@ -364,11 +412,15 @@ extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *f
       return bail(st);
   }
   for (int i = 0; i < count; i++) {
-    if (!S->out[i].ensure(fs)) {
+    if (!S->out[i].ensure(fs) || (S->is_ref[i] && (!S->olp[i].ensure(fs) || !S->oip[i].ensure(fs * 4))) ||
+        (frames[i].intra_mode && !S->init[i].ensure(fs))) {
       c.err = "device allocation failed";
       return bail(DVC_E_NOMEM);
     }
     if ((st = cuda_status(c, cudaMemcpyAsync(S->out[i].p, frames[i].recon, fs, cudaMemcpyHostToDevice, s0), "H2D")))
+      return bail(st);
+    if (frames[i].intra_mode &&
+        (st = cuda_status(c, cudaMemcpyAsync(S->init[i].p, frames[i].recon, fs, cudaMemcpyHostToDevice, s0), "H2D")))
       return bail(st);
   }
   if ((st = cuda_status(c, cudaStreamSynchronize(s0), "session upload"))) return bail(st);
@@ -382,25 +434,59 @@ extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *f
   }
   if ((st = cuda_status(c, cudaEventCreate(&S->t0), "event")) || (st = cuda_status(c, cudaEventCreate(&S->t1), "event")))
     return bail(st);
-  const int nb = (count + max_batch - 1) / max_batch;
+  // batches: level by level, frames of a level in the caller's order, at most
+  // max_batch per batch, streams assigned round-robin
+  const int nlev = *std::max_element(level.begin(), level.end()) + 1;
+  std::vector<int> batch_of(count, -1);
+  for (int lv = 0; lv < nlev; lv++) {
+    std::vector<int> fl;
+    for (int i = 0; i < count; i++)
+      if (level[i] == lv) fl.push_back(i);
+    for (size_t a = 0; a < fl.size(); a += max_batch) {
+      const int b = (int)S->batch_frames.size();
+      S->batch_frames.emplace_back(fl.begin() + a, fl.begin() + std::min(fl.size(), a + (size_t)max_batch));
+      S->batch_stream.push_back(b % nstreams);
+      std::vector<int> deps;
+      for (int i : S->batch_frames[b]) {
+        batch_of[i] = b;
+        for (int k = 0; k < 2; k++)
+          if (dep[i][k] >= 0 && std::find(deps.begin(), deps.end(), batch_of[dep[i][k]]) == deps.end())
+            deps.push_back(batch_of[dep[i][k]]);
+      }
+      S->batch_deps.push_back(deps);
+    }
+  }
+  const int nb = (int)S->batch_frames.size();
   S->batches.resize(nb);
-  S->batch_frames.resize(nb);
   S->results.resize(nb);
   for (int b = 0; b < nb; b++) {
+    cudaEvent_t e;
+    if ((st = cuda_status(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) return bail(st);
+    S->batch_done.push_back(e);
     std::vector<dvc::FrameSpec> specs;
-    for (int i = b * max_batch; i < std::min(count, (b + 1) * max_batch); i++) {
+    for (int i : S->batch_frames[b]) {
       const dvc_wz_frame &f = frames[i];
       dvc::FrameSpec sp;
       sp.w = w;
       sp.h = h;
       sp.qindex = f.qindex;
-      const int pr = refs[f.past], fr = refs[f.future];
-      sp.past = S->ref[pr].as<uint8_t>();
-      sp.future = S->ref[fr].as<uint8_t>();
-      sp.past_lp = S->lp[pr].as<uint8_t>();
-      sp.future_lp = S->lp[fr].as<uint8_t>();
-      sp.past_ip = S->ip[pr].as<uint8_t>();
-      sp.future_ip = S->ip[fr].as<uint8_t>();
+      for (int k = 0; k < 2; k++) {
+        const uint8_t *pl, *pp, *pi;
+        if (dep[i][k] >= 0) {
+          const int d = dep[i][k];
+          pl = S->out[d].as<uint8_t>();
+          pp = S->olp[d].as<uint8_t>();
+          pi = S->oip[d].as<uint8_t>();
+        } else {
+          const int r = refs[k == 0 ? f.past : f.future];
+          pl = S->ref[r].as<uint8_t>();
+          pp = S->lp[r].as<uint8_t>();
+          pi = S->ip[r].as<uint8_t>();
+        }
+        (k == 0 ? sp.past : sp.future) = pl;
+        (k == 0 ? sp.past_lp : sp.future_lp) = pp;
+        (k == 0 ? sp.past_ip : sp.future_ip) = pi;
+      }
       sp.past_idx = f.past_idx;
       sp.future_idx = f.future_idx;
       sp.cur_idx = f.cur_idx;
@@ -412,10 +498,11 @@ extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *f
       sp.acc = f.acc_synd;
       sp.recon = S->out[i].as<uint8_t>();
       specs.push_back(sp);
-      S->batch_frames[b].push_back(i);
     }
-    cudaStream_t sb = S->streams[b % nstreams];
-    if (!S->batches[b].prepare(c, specs, sb)) return bail(DVC_E_CUDA);
+    cudaStream_t sb = S->streams[S->batch_stream[b]];
+    // frames decoding at once: one batch per stream
+    const int concurrent = std::min(count, nstreams * max_batch);
+    if (!S->batches[b].prepare(c, specs, sb, concurrent)) return bail(DVC_E_CUDA);
     if ((st = cuda_status(c, cudaStreamSynchronize(sb), "session prepare"))) return bail(st);
   }
   *out = S;
@@ -426,21 +513,40 @@ extern "C" int dvc_session_run(dvc_session *S, int profile, double *elapsed_ms) 
   if (!S) return DVC_E_ARG;
   Context &c = S->ctx->c;
   const int ns = (int)S->streams.size();
+  const size_t fs = (size_t)S->w * S->h;
   int st;
   cudaStream_t s0 = S->streams[0];
   if ((st = cuda_status(c, cudaEventRecord(S->t0, s0), "event"))) return st;
   for (int k = 1; k < ns; k++)
     if ((st = cuda_status(c, cudaStreamWaitEvent(S->streams[k], S->t0, 0), "wait"))) return st;
-  for (size_t b = 0; b < S->batches.size(); b++)
-    if (!S->batches[b].execute(c, S->streams[b % ns], 50, profile ? &S->prof : nullptr)) return DVC_E_CUDA;
+  for (size_t b = 0; b < S->batches.size(); b++) {
+    cudaStream_t sb = S->streams[S->batch_stream[b]];
+    for (int d : S->batch_deps[b])
+      if ((st = cuda_status(c, cudaStreamWaitEvent(sb, S->batch_done[d], 0), "wait"))) return st;
+    for (int i : S->batch_frames[b])
+      if (S->init[i].p &&
+          (st = cuda_status(c, cudaMemcpyAsync(S->out[i].p, S->init[i].p, fs, cudaMemcpyDeviceToDevice, sb), "D2D")))
+        return st;
+    if (!S->batches[b].execute(c, sb, 50, profile ? &S->prof : nullptr)) return DVC_E_CUDA;
+    // planes of the decoded frames that later levels use as references
+    for (int i : S->batch_frames[b])
+      if (S->is_ref[i] &&
+          (st = cuda_status(c, dvc::launch_ref_planes(S->out[i].as<uint8_t>(), S->w, S->h, S->olp[i].as<uint8_t>(),
+                                                      S->oip[i].as<uint8_t>(), sb),
+                            "reference planes")))
+        return st;
+    if ((st = cuda_status(c, cudaEventRecord(S->batch_done[b], sb), "event"))) return st;
+  }
   for (int k = 1; k < ns; k++) {
     if ((st = cuda_status(c, cudaEventRecord(S->done[k], S->streams[k]), "event"))) return st;
     if ((st = cuda_status(c, cudaStreamWaitEvent(s0, S->done[k], 0), "wait"))) return st;
   }
   if ((st = cuda_status(c, cudaEventRecord(S->t1, s0), "event"))) return st;
   for (size_t b = 0; b < S->batches.size(); b++)
-    if (!S->batches[b].collect(c, S->results[b], S->streams[b % ns])) return DVC_E_CUDA;
+    if (!S->batches[b].collect(c, S->results[b], S->streams[S->batch_stream[b]])) return DVC_E_CUDA;
   if ((st = cuda_status(c, cudaEventSynchronize(S->t1), "session run"))) return st;
+  for (int k = 0; k < ns; k++)
+    if ((st = cuda_status(c, cudaStreamSynchronize(S->streams[k]), "session collect"))) return st;
   if (profile)
     for (auto &b : S->batches) b.harvest(&S->prof);
   float ms = 0;

@@ -82,6 +82,7 @@ bool Context::init(const char *data, const char *tables, int dev) {
   xlm.exp_mask = xlm_host.hdr.exp_cap - 1;
   xlm.log_shift = 32 - lg2(xlm_host.hdr.log_cap);
   xlm.exp_shift = 32 - lg2(xlm_host.hdr.exp_cap);
+  xlm.exp_tie = xlm_host.hdr.exp_tie;
   xlm.tanh_ylo = xlm_host.hdr.tanh_ylo;
   xlm.tanh_y1 = xlm_host.hdr.tanh_y1;
   {

@@ -70,8 +70,11 @@ __device__ __forceinline__ float xl_expf(const XlmDev &t, const XlSmall &s, floa
   const uint32_t u = __float_as_uint(x);
   if (x != x) return x;
   if (u >= XL_EXP_HI && (u >> 31)) return 0.0f;  // x <= -104 (and -inf): underflows to +0
-  const float m = xl_expf_base(x, s);
+  const double d = xl_exp_d((double)x, s);
+  const float m = XL_D2F(d);
   if (!(u >> 31)) return m;  // positive arguments do not occur in the decoder
+  // every exception with a normal result lies within exp_tie of a midpoint
+  if (d >= 0x1p-126 && xl_tie_dist(d) > t.exp_tie) return m;
   return xl_hash_lookup(t.exp_tab, t.exp_mask, t.exp_shift, u, m);
 }
 

@@ -26,7 +26,10 @@
 //     except in rare near-tie cases.
 //  2. Correction tables built on the host by sweeping the C library over the
 //     exact input domain (libm_tables.cpp): the inputs where the library's float
-//     result differs from part 1, with the library's value, in a hash.
+//     result differs from part 1, with the library's value, in a hash.  For
+//     expf every such input lies within a tiny distance of a float rounding
+//     midpoint (the sweep records the largest, exp_tie); the device reads the
+//     hash only for results that close to a midpoint (about 1 in 10^5).
 //
 // The belief-propagation magnitude phi(y) = -logf(tanhf(y)) is not evaluated
 // at all: its argument is a float in [2^-31, y1) (y1 = the first float with
@@ -130,6 +133,16 @@ XL_HD double xl_log_d(double x, const XlSmall &s) {
 // float results of part 1, before corrections
 XL_HD float xl_expf_base(float x, const XlSmall &s) { return XL_D2F(xl_exp_d((double)x, s)); }
 XL_HD float xl_logf_base(float x, const XlSmall &s) { return XL_D2F(xl_log_d((double)x, s)); }
+
+// Distance of a double from the nearest float rounding boundary (the midpoint
+// between two floats of its binade), in units of 2^-52 of the binade: the
+// 29 mantissa bits that rounding to float drops, measured from 2^28.  A
+// library whose float result differs from the correctly rounded one only for
+// doubles this close to a midpoint agrees with XL_D2F(d) everywhere else.
+XL_HD uint32_t xl_tie_dist(double d) {
+  const uint32_t low = (uint32_t)(xl_dbits(d) & ((1u << 29) - 1));
+  return low >= (1u << 28) ? low - (1u << 28) : (1u << 28) - low;
+}
 
 // ---- domains (float bit patterns, inclusive) swept by the table builder ----
 // logf inputs: LLR from LR in [1e-4/0.9999, 0.9999/1e-4], tanh values in

@@ -25,10 +25,23 @@ namespace dvc {
 __constant__ double c_post_scale[16];
 __constant__ double c_pre_scale[16];
 
+// updateSI motion-vector weight 1 + 0.05f * |2v| per integer displacement
+// (dx, dy) in [-32, 32]^2 (sideInfoCreation.cpp:667-668), indexed
+// (dy + 32) * 65 + dx + 32
+__device__ double d_si_weight[65 * 65];
+
 cudaError_t upload_transform_scales(const double *post, const double *pre) {
   cudaError_t e = cudaMemcpyToSymbol(c_post_scale, post, sizeof(double) * 16);
   if (e != cudaSuccess) return e;
-  return cudaMemcpyToSymbol(c_pre_scale, pre, sizeof(double) * 16);
+  if ((e = cudaMemcpyToSymbol(c_pre_scale, pre, sizeof(double) * 16)) != cudaSuccess) return e;
+  // IEEE square root on the host gives the device's bits (no contraction: -ffp-contract=off)
+  static double wt[65 * 65];
+  for (int dy = -32; dy <= 32; dy++)
+    for (int dx = -32; dx <= 32; dx++) {
+      const double vx = (double)(dx << 1), vy = (double)(dy << 1);
+      wt[(dy + 32) * 65 + dx + 32] = 1.0 + (double)0.05f * sqrt(vx * vx + vy * vy);
+    }
+  return cudaMemcpyToSymbol(d_si_weight, wt, sizeof wt);
 }
 
 // Does the frame take part in step (band, bit)?  band < 0: frame-level steps.
@@ -637,20 +650,24 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
     return;
   }
   const float a = F.alpha[(top + (index >> 2)) * w + left + (index & 3)];
-  if (threadIdx.x == 0) {
-    const Win wn = ml_window(top, left, w, h);
-    int q = 0, mx = 0;
-    for (int m = wn.st; m <= wn.sb; m++)
-      for (int n = wn.sl; n <= wn.sr; n++) {
-        const int v = F.oct[((size_t)m * srw + n) * 16 + index];
-        sc[q] = v;
-        prob[q] = F.smf[(size_t)s_idx * ML_N + q];
-        mx = max(mx, abs(v));
-        q++;
-      }
-    s_n = q;
-    s_dmax = range + mx;
+  // the SMF candidates in row-major window order, gathered in parallel
+  const Win wn = ml_window(top, left, w, h);
+  const int cw = wn.sr - wn.sl + 1, ncand = cw * (wn.sb - wn.st + 1);
+  if (threadIdx.x == 0) s_dmax = 0;
+  __syncthreads();
+  int mx = 0;
+  for (int q = threadIdx.x; q < ncand; q += NT) {
+    const int m = wn.st + q / cw, n = wn.sl + q % cw;
+    const int v = F.oct[((size_t)m * srw + n) * 16 + index];
+    sc[q] = v;
+    prob[q] = F.smf[(size_t)s_idx * ML_N + q];
+    mx = max(mx, abs(v));
   }
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&s_dmax, mx);
+  if (threadIdx.x == 0) s_n = ncand;
+  __syncthreads();
+  if (threadIdx.x == 0) s_dmax += range;
   __syncthreads();
   const int nm = s_n, dmax = s_dmax;
   const int tab = dmax < NOISE_TAB ? dmax + 1 : NOISE_TAB;
@@ -805,38 +822,66 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   if (sl < 0) sl = 0;
   if (sr > w - 4) sr = w - 4;
   const int ww = sr - sl + 4, wh = sb - st + 4;  // <= 68 x 68
-  __shared__ uint8_t wp[68 * 68], wf[68 * 68];
+  // windows with a 72-byte row stride, so that the word after any 4-byte
+  // group of a row is still inside the row
+  constexpr int WS = 72;
+  __shared__ __align__(16) uint8_t wp[68 * WS], wf[68 * WS];
+  __shared__ uint32_t cur4[4];  // the block's rows, 4 pixels packed per word (first pixel lowest)
   __shared__ int cur[16];
   __shared__ double scp[NT / 32], scf[NT / 32];
   __shared__ int sip[NT / 32], sif[NT / 32];
   for (int k = threadIdx.x; k < ww * wh; k += NT) {
     const int y = k / ww, x = k - y * ww;
-    wp[k] = F.past[(st + y) * w + sl + x];
-    wf[k] = F.future[(st + y) * w + sl + x];
+    wp[y * WS + x] = F.past[(st + y) * w + sl + x];
+    wf[y * WS + x] = F.future[(st + y) * w + sl + x];
   }
   if (threadIdx.x < 16) cur[threadIdx.x] = F.recon[(top + (threadIdx.x >> 2)) * w + left + (threadIdx.x & 3)];
   __syncthreads();
-  const int cw = sr - sl + 1, nc = cw * (sb - st + 1);
+  if (threadIdx.x < 4) {
+    const int m = threadIdx.x;
+    cur4[m] = (uint32_t)cur[4 * m] | ((uint32_t)cur[4 * m + 1] << 8) | ((uint32_t)cur[4 * m + 2] << 16) |
+              ((uint32_t)cur[4 * m + 3] << 24);
+  }
+  __syncthreads();
+  // one thread per (reference, candidate column): the SAD of candidate row yo
+  // is the sum over m of the 4-pixel SAD of window row yo + m against block
+  // row m, accumulated while walking the window rows once
+  const int cw = sr - sl + 1;
   double bp = 1e300, bf = 1e300;
   int ip = 0x7fffffff, jf = 0x7fffffff;
-  for (int c = threadIdx.x; c < nc; c += NT) {
-    const int yo = c / cw, xo = c - yo * cw;
-    int sp = 0, sf = 0;
+  const uint32_t c0 = cur4[0], c1 = cur4[1], c2 = cur4[2], c3 = cur4[3];
+  for (int pc = threadIdx.x; pc < 2 * cw; pc += NT) {
+    const bool fut = pc >= cw;
+    const int xo = fut ? pc - cw : pc;
+    const uint8_t *wb = fut ? wf : wp;
+    const uint32_t *row = reinterpret_cast<const uint32_t *>(wb) + (xo >> 2);
+    const int sh = (xo & 3) * 8;
+    const double *wt = d_si_weight + (st - top + 32) * 65 + (sl + xo - left + 32);
+    int part[4] = {0, 0, 0, 0};  // running SADs of candidate rows y-3 .. y (indexed by row & 3)
+    for (int y0 = 0; y0 < wh; y0 += 4) {
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-      const int base = (yo + m) * ww + xo;
-#pragma unroll
-      for (int n = 0; n < 4; n++) {
-        const int b = cur[4 * m + n];
-        sp += abs(b - (int)wp[base + n]);
-        sf += abs(b - (int)wf[base + n]);
+      for (int r = 0; r < 4; r++) {
+        const int y = y0 + r;
+        if (y < wh) {
+          const uint32_t *rw = row + y * (WS / 4);
+          const uint32_t v = __funnelshift_r(rw[0], rw[1], sh);
+          // window row y is row m of candidate y - m
+          part[(r - 0) & 3] = (int)__vsadu4(v, c0);
+          part[(r - 1) & 3] += (int)__vsadu4(v, c1);
+          part[(r - 2) & 3] += (int)__vsadu4(v, c2);
+          part[(r - 3) & 3] += (int)__vsadu4(v, c3);
+          const int yo = y - 3;
+          if (yo >= 0) {
+            const int sad = part[(r - 3) & 3];
+            const double cst = (double)sad * __ldg(wt + yo * 65);
+            if (cst < 10000000.0) {
+              if (fut) better(bf, jf, cst, yo * cw + xo);
+              else better(bp, ip, cst, yo * cw + xo);
+            }
+          }
+        }
       }
     }
-    const double vx = (double)((sl + xo - left) << 1), vy = (double)((st + yo - top) << 1);
-    const double wgt = 1.0 + (double)0.05f * sqrt(vx * vx + vy * vy);
-    const double cp = (double)sp * wgt, cf = (double)sf * wgt;
-    if (cp < 10000000.0) better(bp, ip, cp, c);
-    if (cf < 10000000.0) better(bf, jf, cf, c);
   }
   block_argmin<NT>(bp, ip, scp, sip);
   block_argmin<NT>(bf, jf, scf, sif);

@@ -112,15 +112,22 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
   std::vector<Pair> logp;
   for (auto &v : parts) { logp.insert(logp.end(), v.begin(), v.end()); v.clear(); }
 
-  // ---- expf over [-104, -0]
+  // ---- expf over [-104, -0], and the largest midpoint distance of an
+  //      exception whose result is a normal float
+  std::vector<uint32_t> tie(threads, 0);
   parallel_ranges(XL_EXP_LO, XL_EXP_HI, threads, [&](int t, uint64_t a, uint64_t b) {
     auto &v = parts[t];
     for (uint64_t u = a; u <= b; u++) {
       const float x = xl_bitsf((uint32_t)u);
+      const double d = xl_exp_d((double)x, sv);
       const float g = expf(x), m = xl_expf_base(x, sv);
-      if (xl_fbits(g) != xl_fbits(m)) v.push_back({(uint32_t)u, xl_fbits(g)});
+      if (xl_fbits(g) != xl_fbits(m)) {
+        v.push_back({(uint32_t)u, xl_fbits(g)});
+        if (d >= 0x1p-126) tie[t] = std::max(tie[t], xl_tie_dist(d));
+      }
     }
   });
+  const uint32_t exp_tie = *std::max_element(tie.begin(), tie.end());
   std::vector<Pair> expp;
   for (auto &v : parts) { expp.insert(expp.end(), v.begin(), v.end()); v.clear(); }
 
@@ -160,6 +167,7 @@ extern "C" int dvc_libm_build(const char *path, int threads, char *err, int errl
   h.exp_count = (uint32_t)expp.size();
   h.tanh_ylo = XL_TANH_YLO;
   h.tanh_y1 = y1;
+  h.exp_tie = exp_tie;
   std::string tmp = std::string(path) + ".tmp";
   FILE *f = fopen(tmp.c_str(), "wb");
   if (!f) {

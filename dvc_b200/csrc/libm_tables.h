@@ -6,7 +6,7 @@
 #include <vector>
 #endif
 
-#define XLM_MAGIC "DVCXLM03"
+#define XLM_MAGIC "DVCXLM04"
 
 typedef struct {
   char magic[8];
@@ -14,7 +14,8 @@ typedef struct {
   uint32_t log_cap, log_count;  // logf hash: log_cap (key, value) slots, power of two
   uint32_t exp_cap, exp_count;  // expf hash
   uint32_t tanh_ylo, tanh_y1;   // tanh argument range [ylo, y1) of the phi table; y >= y1 gives tanhf 1
-  uint32_t reserved[8];
+  uint32_t exp_tie;             // largest xl_tie_dist of an expf exception with a normal result
+  uint32_t reserved[7];
 } XlmHeader;
 
 // small tables of the base functions (exact_libm.h); stored after the big ones
@@ -33,6 +34,7 @@ typedef struct {
   uint32_t log_mask, exp_mask;  // cap - 1
   int log_shift, exp_shift;     // 32 - log2(cap)
   uint32_t tanh_ylo, tanh_y1;
+  uint32_t exp_tie;
   const XlmSmallTables *small;  // device copy
 } XlmDev;
 

@@ -172,17 +172,23 @@ class Context:
         return dec, rate.value, lr
 
     def _frame_array(self, items):
+        """ctypes frame array.  An item may name another item's decoded output as
+        a reference with past_from / future_from (its index); the pointer then
+        equals that item's recon pointer, which dvc_session_create resolves."""
         keep, arr, outs = [], (WZFrame * len(items))(), []
+        recs = [np.zeros((it["height"], it["width"]), np.uint8) if it.get("recon") is None else
+                np.ascontiguousarray(it["recon"], np.uint8).copy() for it in items]
         for i, it in enumerate(items):
             w, h = it["width"], it["height"]
-            past = np.ascontiguousarray(it["past"], np.uint8)
-            fut = np.ascontiguousarray(it["future"], np.uint8)
+            past = recs[it["past_from"]] if it.get("past_from") is not None else \
+                np.ascontiguousarray(it["past"], np.uint8)
+            fut = recs[it["future_from"]] if it.get("future_from") is not None else \
+                np.ascontiguousarray(it["future"], np.uint8)
             mode = None if it.get("mode") is None else np.ascontiguousarray(it["mode"], np.uint8)
             acr = np.ascontiguousarray(it["ac_range"], np.int32)
             crc = np.ascontiguousarray(it["crc"], np.uint8)
             acc = np.ascontiguousarray(it["acc"], np.uint8)
-            rec = np.zeros((h, w), np.uint8) if it.get("recon") is None else \
-                np.ascontiguousarray(it["recon"], np.uint8).copy()
+            rec = recs[i]
             keep += [past, fut, mode, acr, crc, acc, rec]
             arr[i] = WZFrame(w, h, it["qindex"], it["past_idx"], it["future_idx"], it["cur_idx"], _ptr(past),
                              _ptr(fut), _ptr(mode), it.get("skip_mode", 0), it.get("intra_mode", 0), _ptr(acr),
@@ -198,7 +204,8 @@ class Context:
         return srv
 
     def session(self, items, max_batch=0, streams=1):
-        """Device-resident session over independent frames (dvc_session_*)."""
+        """Device-resident session (dvc_session_*); items may reference each
+        other's outputs through past_from / future_from."""
         return Session(self, items, max_batch, streams)
 
     def debug_wz_frame(self, item):

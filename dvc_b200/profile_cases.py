@@ -1,7 +1,7 @@
 """Small, self-contained GPU workloads for profiler captures.
 
     python -m dvc_b200.profile_cases ldpca-cif     # LDPCA ladder on the 11 CIF golden bitplanes
-    python -m dvc_b200.profile_cases frame-cif     # one CIF WZ frame (Q4) through every kernel
+    python -m dvc_b200.profile_cases frame-cif [Q] # one CIF WZ frame (QIndex Q, default 4) through every kernel
 
 Each case runs once after one warm-up run, so a profiler can skip the warm-up
 launches and capture the second instance of a kernel.
@@ -21,10 +21,10 @@ def ldpca_cif(ctx):
     assert np.array_equal(res[:, 0], g["rate"])
 
 
-def frame_cif(ctx):
+def frame_cif(ctx, q=4):
     from . import bitstream as bs, decoder, encoder, synth
     ori, key = synth.make_sequence("cif", 3, 101)
-    st = bs.parse_wz(encoder.encode_sequence(ori, 2, 4))
+    st = bs.parse_wz(encoder.encode_sequence(ori, 2, q))
     m, b, e = bs.sequence_order(st.n_frames, st.gop)[0]
     it = decoder.frame_item(st, st.frames[m], key)
     for _ in range(2):
@@ -38,7 +38,7 @@ def main():
     from . import native
     name = sys.argv[1] if len(sys.argv) > 1 else "ldpca-cif"
     ctx = native.Context(0)
-    CASES[name](ctx)
+    CASES[name](ctx, *[int(a) for a in sys.argv[2:]])
     ctx.close()
     print("case", name, "done")
 

@@ -135,9 +135,13 @@ int dvc_ldpca_decode_noalloc(dvc_ctx *ctx, int n, int count, const float *d_lr, 
  * are uploaded once by dvc_session_create; every dvc_session_run decodes all
  * of them again from device memory, in batches of at most `max_batch` frames
  * spread over `streams` concurrent CUDA streams, and keeps the results on the
- * device until dvc_session_frame copies them out.  Frames of one session must
- * share one size and be independent of each other.  No counterpart in the
- * reference (its GPU path copies every stage's data in and out). */
+ * device until dvc_session_frame copies them out.  Frames of one session share
+ * one size.  A frame whose past or future pointer equals another frame's
+ * recon pointer takes that frame's decoded output as the reference (the GOP
+ * recursion of DVC_Decoder.cpp:26-474 for GOP 4 and 8): frames are grouped
+ * into levels and a batch starts when the batches it reads from are done,
+ * with no host round trip.  No counterpart in the reference (its GPU path
+ * copies every stage's data in and out). */
 typedef struct dvc_session dvc_session;
 int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *frames, int max_batch, int streams,
                        dvc_session **out);

@@ -46,3 +46,34 @@ def test_first_frame_stages_match_oracle(gpu_ctx, golden_dir, seq):
     assert np.array_equal(out["planes"][:, 2], ref["accepted"]), "accepted codes"
     assert np.array_equal(out["si_final"], ref["si_final"]), "refined side information"
     assert np.array_equal(out["recon"], ref["recon"]), "decoded frame"
+
+
+@pytest.mark.parametrize("seq", ["qcif_g4_q8"])
+def test_session_levels_match_reference(gpu_ctx, golden_dir, seq):
+    """A GOP-4 sequence as one device-resident session: frames 1 and 3 of each GOP
+    name frame 2's decoded output as their reference (past_from / future_from),
+    so the second level starts on the device without a host round trip; run twice."""
+    g = np.load(os.path.join(golden_dir, f"seq_{seq}.npz"))
+    ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
+    st = bs.parse_wz(g["wz"].tobytes())
+    items, where = [], {}
+    for lvl in decoder.decode_levels(st):
+        for (m, b, e) in lvl:
+            it = decoder.frame_item(st, st.frames[m], key)
+            for name, ref in (("past", b), ("future", e)):
+                if ref in st.frames:
+                    it[name + "_from"], it[name] = where[ref], None
+            where[m] = len(items)
+            items.append(it)
+    assert any(it.get("past_from") is not None or it.get("future_from") is not None for it in items)
+    ses = gpu_ctx.session(items, max_batch=3, streams=2)
+    try:
+        for _ in range(2):
+            ses.run()
+            for m, i in where.items():
+                rec, bits, planes = ses.frame(i)
+                assert np.array_equal(rec, g["dec_y"][m]), f"frame {m} Y differs"
+                k = list(g["frames"]).index(m)
+                assert bits == g["bits"][k] - st.frames[m].skip_bits - st.frames[m].intra_map_bits
+    finally:
+        ses.close()

@@ -27,11 +27,10 @@ def test_server_mix_matches_alone(gpu_ctx):
     # staggered arrivals: half now, the rest while the first cohorts are decoding
     for it in mix[: len(mix) // 2]:
         tickets.append(srv.submit(it))
-    srv.poll()
+    done = srv.poll()
     for it in mix[len(mix) // 2:]:
         tickets.append(srv.submit(it))
-        srv.poll()
-    done = 0
+        done += srv.poll()
     t0 = time.time()
     while done < len(mix) and time.time() - t0 < 120:
         done += srv.poll()
