@@ -270,6 +270,7 @@ def main():
                     for name, d in zip(("past", "future"), deps):
                         if d is not None:
                             it[name] = res[d]["recon"]
+                            it.pop(name + "_from")
                 tickets[srv.submit(it)] = i
             waiting = still
             if srv.poll():
@@ -329,13 +330,18 @@ def main():
         plain_lat.append(time.perf_counter() - t0)
     plain_fps = len(plain_lat) / sum(plain_lat)
 
-    # roofline of the dominant kernel (LDPCA ladder): algorithmic bytes per codeword
-    # = LR in (4n) + accumulated syndrome (n/8) + quantisation indices read+written (8n) + result
-    n = fs // 16
-    alg_bytes_cw = 4 * n + n // 8 + 8 * n + 20
+    # roofline of the dominant kernel (the LDPCA ladder).  Unit: one belief-
+    # propagation iteration of one thread block on a CIF codeword; its
+    # algorithmic DRAM bytes are the phi-table reads, one 4-byte entry per edge
+    # in each of the two message passes (2 * 19008 * 4); messages, signs and
+    # row sums stay in shared memory.
+    E_CIF = 19008
+    alg_bytes_unit = 2 * E_CIF * 4
     ld_avg_ms = prof["ldpca_ms"] / max(1, prof["ldpca_launches"])
     cw_per_launch = prof["ldpca_codewords"] / max(1, prof["ldpca_launches"])
-    achieved = alg_bytes_cw * cw_per_launch / (ld_avg_ms / 1e3) / 1e9
+    units_per_launch = bp_iters / max(1, prof["ldpca_launches"])
+    achieved = alg_bytes_unit * units_per_launch / (ld_avg_ms / 1e3) / 1e9
+    aggregate = alg_bytes_unit * bp_iters / (step_ms / 1e3) / 1e9
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
@@ -343,9 +349,9 @@ def main():
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "ldpca_traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("bytes_per_codeword")
-        if traffic is not None:
-            traffic = traffic * cw_per_launch
+        per_unit = json.load(open(tpath)).get("dram_bytes_per_block_iteration")
+        if per_unit is not None:
+            traffic = per_unit * units_per_launch
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -382,10 +388,16 @@ def main():
                            streams=args.streams, max_cohort=args.max_batch, sweep=served_sweep),
             "roofline": {"bound": "hbm", "kernel": "ldpca_ladder_kernel", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                         "note": "path is FP64/latency bound: exact C-library logf/tanhf per edge"},
+                         "unit_of_work": "BP block-iteration on a CIF codeword, %d algorithmic bytes (phi-table "
+                                         "reads)" % alg_bytes_unit,
+                         "units_per_launch": units_per_launch,
+                         "aggregate_achieved": aggregate, "aggregate_frac": aggregate / peak,
+                         "note": "4-byte random gathers from a 1.1 GB table; each costs a 32-byte DRAM sector, "
+                                 "and launches of 16 streams overlap, so the per-launch figure understates the "
+                                 "device-wide rate (aggregate_achieved: all launches of a step over the step time)"},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
-            "gpu_launches": int(prof["kernel_launches"] / max(1, prof["runs"]) * args.steps),
+            "gpu_launches": int(prof["kernel_launches"]) * args.steps,
             "ldpca": {"ms_per_launch": ld_avg_ms, "codewords_per_launch": cw_per_launch,
                       "kernel_ms_per_step": prof["ldpca_ms"],
                       "bp_block_iterations_per_step": bp_iters,

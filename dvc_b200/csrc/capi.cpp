@@ -529,12 +529,14 @@ extern "C" int dvc_session_run(dvc_session *S, int profile, double *elapsed_ms) 
         return st;
     if (!S->batches[b].execute(c, sb, 50, profile ? &S->prof : nullptr)) return DVC_E_CUDA;
     // planes of the decoded frames that later levels use as references
-    for (int i : S->batch_frames[b])
-      if (S->is_ref[i] &&
-          (st = cuda_status(c, dvc::launch_ref_planes(S->out[i].as<uint8_t>(), S->w, S->h, S->olp[i].as<uint8_t>(),
+    for (int i : S->batch_frames[b]) {
+      if (!S->is_ref[i]) continue;
+      if ((st = cuda_status(c, dvc::launch_ref_planes(S->out[i].as<uint8_t>(), S->w, S->h, S->olp[i].as<uint8_t>(),
                                                       S->oip[i].as<uint8_t>(), sb),
                             "reference planes")))
         return st;
+      if (profile) S->prof.kernel_launches += 2;  // low-pass and half-pel kernels
+    }
     if ((st = cuda_status(c, cudaEventRecord(S->batch_done[b], sb), "event"))) return st;
   }
   for (int k = 1; k < ns; k++) {

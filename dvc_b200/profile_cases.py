@@ -2,6 +2,7 @@
 
     python -m dvc_b200.profile_cases ldpca-cif     # LDPCA ladder on the 11 CIF golden bitplanes
     python -m dvc_b200.profile_cases frame-cif [Q] # one CIF WZ frame (QIndex Q, default 4) through every kernel
+    python -m dvc_b200.profile_cases ldpca-micro   # 148 CIF codewords of the LDPCA microbenchmark, one launch
 
 Each case runs once after one warm-up run, so a profiler can skip the warm-up
 launches and capture the second instance of a kernel.
@@ -31,7 +32,16 @@ def frame_cif(ctx, q=4):
         ctx.decode_wz_frames([it])
 
 
-CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif}
+def ldpca_micro(ctx, count=148):
+    from . import ldpca_bench as lb
+    lr, acc, crc, x = lb.make_codewords(6336, count, 5)
+    for _ in range(2):
+        dec, res, ent = ctx.ldpca_decode(lr, acc, crc)
+    assert np.array_equal(dec, x)
+    print("bp block-iterations per launch", int(res[:, 3].sum()))
+
+
+CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif, "ldpca-micro": ldpca_micro}
 
 
 def main():
