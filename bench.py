@@ -223,11 +223,8 @@ def main():
             dev_ms.append(ses.run(profile=(i == args.steps - 1)))
         barrier()
     prof = ses.profile()
-    step_ms = float(np.mean(dev_ms))
-    if world > 1:
-        t = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
+    from dvc_b200 import replicas
+    step_ms = replicas.max_over_ranks(float(np.mean(dev_ms)))
     frames_per_step = len(its)
     value = world * frames_per_step / (step_ms / 1e3)
 
@@ -296,11 +293,7 @@ def main():
         dt, _, served = serve_all()
         e2e_t.append(dt)
     barrier()
-    e2e_s = float(np.mean(e2e_t))
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(float(np.mean(e2e_t)))
     # the served results equal the session's (both bit-exact paths), second level included
     for i in (0, len(its) // 2, len(its) - 1, max(i for i in range(len(its)) if lev[i] > 0)):
         rec_i, bits_i, _ = ses.frame(i)

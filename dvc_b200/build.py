@@ -1,6 +1,7 @@
 """Build libdvc_b200.so in-tree for sm_100a.
 
-    python -m dvc_b200.build            # compile every csrc/*.cu, *.cpp and link
+    python -m dvc_b200.build            # compile every csrc/*.cu, *.cpp and link,
+                                        # then the dvcdec executable (cli/dvcdec.cpp)
 
 Every CUDA translation unit is compiled with -fmad=false (no contraction of
 a*b+c into fused multiply-adds, matching the reference's x86 SSE2 arithmetic)
@@ -18,6 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libdvc_b200.so")
+CLI_SRC = os.path.join(HERE, "cli", "dvcdec.cpp")
+CLI = os.path.join(LIBDIR, "dvcdec")
 ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -60,13 +63,26 @@ def build(verbose=False, ptxas_info=False):
     extra = ["-Xptxas", "-v"] if ptxas_info else []
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose or ptxas_info, extra), sources()))
-    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
-        return LIB
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"]
+    if not (os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs)):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+    build_cli()
+    return LIB
+
+
+def build_cli():
+    """The DvcDec-compatible executable, linked against the library beside it."""
+    hdr = os.path.join(ROOT, "include", "dvc_b200.h")
+    if os.path.exists(CLI) and os.path.getmtime(CLI) >= max(os.path.getmtime(p) for p in (CLI_SRC, hdr, LIB)):
+        return CLI
+    cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), CLI_SRC,
+           "-L", LIBDIR, "-ldvc_b200", "-Wl,-rpath,$ORIGIN", "-o", CLI]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("link failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
-    return LIB
+        raise RuntimeError("dvcdec build failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+    return CLI
 
 
 if __name__ == "__main__":

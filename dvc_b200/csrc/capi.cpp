@@ -132,6 +132,36 @@ extern "C" int dvc_ldpca_decode(dvc_ctx *ctx, int n, int count, const float *lr,
   return ldpca_run(ctx->c, n, count, lr, acc, crc, decoded, results, entropy, max_iter, nullptr, nullptr);
 }
 
+extern "C" int dvc_ldpca_encode(dvc_ctx *ctx, int n, int count, const uint8_t *bits, uint8_t *acc, uint8_t *crc) {
+  if (!ctx) return DVC_E_ARG;
+  Context &c = ctx->c;
+  const dvc::LadderDev *L = c.ladder(n);
+  if (!L) {
+    c.err = "no ladder for codeword length " + std::to_string(n);
+    return DVC_E_ARG;
+  }
+  if (count <= 0 || !bits || !acc || !crc) {
+    c.err = "dvc_ldpca_encode: bad arguments";
+    return DVC_E_ARG;
+  }
+  const size_t nb = (size_t)n / 8;
+  if (!c.ld_dec.ensure((size_t)count * n) || !c.ld_acc.ensure((size_t)count * nb) || !c.ld_res.ensure((size_t)count)) {
+    c.err = "device allocation failed";
+    return DVC_E_NOMEM;
+  }
+  cudaStream_t s = c.stream;
+  int st;
+  if ((st = cuda_status(c, cudaMemcpyAsync(c.ld_dec.p, bits, (size_t)count * n, cudaMemcpyHostToDevice, s), "H2D bits")) ||
+      (st = cuda_status(c, dvc::launch_ldpca_encode(*L, c.ld_dec.as<uint8_t>(), count, c.ld_acc.as<uint8_t>(),
+                                                    c.ld_res.as<uint8_t>(), s),
+                        "ldpca encode")) ||
+      (st = cuda_status(c, cudaMemcpyAsync(acc, c.ld_acc.p, (size_t)count * nb, cudaMemcpyDeviceToHost, s), "D2H acc")) ||
+      (st = cuda_status(c, cudaMemcpyAsync(crc, c.ld_res.p, (size_t)count, cudaMemcpyDeviceToHost, s), "D2H crc")) ||
+      (st = cuda_status(c, cudaStreamSynchronize(s), "ldpca encode sync")))
+    return st;
+  return DVC_OK;
+}
+
 extern "C" int dvc_LdpcaDecoder(dvc_ctx *ctx, int n, float *LR_intrinsic, const unsigned char *accumulatedSyndrome,
                                 unsigned char *decoded, int *rate, unsigned char crc_encoder, float RateLowerBound) {
   if (!ctx || !LR_intrinsic || !accumulatedSyndrome || !decoded || !rate || (n & 7)) return DVC_E_ARG;

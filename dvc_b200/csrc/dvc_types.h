@@ -25,6 +25,7 @@ struct LadderDev {
   // in increasing e, rows in order.
   const uint16_t *pos;       // [num_codes*e] row-order position of edge e
   const uint16_t *rid;       // [num_codes*e] row of row-order position p
+  const uint16_t *ir_full;   // [e] row of edge e in the full-rate code (the encoder's matrix)
   const uint8_t *crc_tab;    // [n]
   const uint32_t *invh;      // [n*invh_words]
 };

@@ -18,5 +18,8 @@ LdpcaSpec ldpca_spec_carve(void *base, int num_jobs, int K);
 cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
                               int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream);
 void set_ldpca_threads(int nt);
+// encoder: accumulated syndromes (n/8 bytes, MSB first) and CRC-8 of `count` source bitplanes
+cudaError_t launch_ldpca_encode(const LadderDev &L, const uint8_t *bits_dev, int count, uint8_t *acc_dev,
+                                uint8_t *crc_dev, cudaStream_t stream);
 
 }  // namespace dvc

@@ -55,6 +55,7 @@ bool load_ladders(const std::string &path, std::vector<LadderHost> &out, std::st
     if (!rd(f, jc16.data(), 2 * jc16.size()) || !rd(f, ir16.data(), 2 * ir16.size())) break;
     L.jc.assign(jc16.begin(), jc16.end());
     L.ir_full.assign(ir16.begin(), ir16.end());
+    L.ir_full16 = ir16;
     L.bpp.resize(L.num_codes);
     L.idx.assign((size_t)L.num_codes * L.period, 0);
     for (int c = 0; c < L.num_codes; c++) {
@@ -245,7 +246,7 @@ bool LadderGpu::upload(const LadderHost &L, std::string &err) {
   return put(allocs, L.jc, &dev.jc, err) && put(allocs, L.bpp, &dev.bpp, err) && put(allocs, L.idx, &dev.idx, err) &&
          put(allocs, L.synd_len, &dev.synd_len, err) && put(allocs, L.code_rate, &dev.code_rate, err) &&
          put(allocs, L.row_ptr, &dev.row_ptr, err) && put(allocs, L.pos, &dev.pos, err) &&
-         put(allocs, L.rid, &dev.rid, err) &&
+         put(allocs, L.rid, &dev.rid, err) && put(allocs, L.ir_full16, &dev.ir_full, err) &&
          put(allocs, L.crc_tab, &dev.crc_tab, err) && put(allocs, L.invh, &dev.invh, err);
 }
 

@@ -18,6 +18,7 @@ struct LadderHost {
   std::vector<uint8_t> crc_tab;
   std::vector<uint32_t> invh;
   std::vector<int> ir_full;  // full-rate rows (the encoder's parity-check matrix)
+  std::vector<uint16_t> ir_full16;
 };
 
 // Reads every ladder in `path` (layout documented in ladders/ladders.py).

@@ -92,6 +92,7 @@ FRAME_API = {
     "dvc_ldpca_decode_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
+    "dvc_ldpca_encode": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p],
 }
 
 
@@ -157,6 +158,17 @@ class Context:
                                               C.c_void_p(d_crc), C.c_void_p(d_decoded) if d_decoded else None,
                                               C.c_void_p(d_results), C.c_void_p(d_entropy) if d_entropy else None,
                                               max_iter, C.c_void_p(stream) if stream else None)
+
+    def ldpca_encode(self, bits):
+        """Device LDPCA encoder. bits: (count, n) 0/1. Returns (accumulated syndrome bytes (count, n/8), crc (count,))."""
+        bits = np.ascontiguousarray(bits, np.uint8)
+        if bits.ndim == 1:
+            bits = bits[None]
+        count, n = bits.shape
+        acc = np.zeros((count, n // 8), np.uint8)
+        crc = np.zeros(count, np.uint8)
+        self.check(lib().dvc_ldpca_encode(self._h, n, count, _ptr(bits), _ptr(acc), _ptr(crc)))
+        return acc, crc
 
     def last_error(self):
         return lib().dvc_last_error(self._h).decode()

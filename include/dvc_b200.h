@@ -59,6 +59,14 @@ const char *dvc_last_error(dvc_ctx *ctx);
 int dvc_ldpca_decode(dvc_ctx *ctx, int n, int count, const float *lr, const uint8_t *acc, const uint8_t *crc,
                      uint8_t *decoded, int *results, float *entropy, int max_iter);
 
+/* LDPCA encoder on the device: for `count` source bitplanes of n bits
+ * (bits[count*n], one 0/1 byte per bit) the accumulated syndromes acc[count*n/8]
+ * (full-rate syndrome H*x, prefix-xored over the rows, packed MSB first as in
+ * the WZ bitstream) and crc[count] (CRC-8 of the bitplane).  Equivalent to
+ * LdpcaEncoder (DvcEnc/src/LdpcaEncoder.cpp:64-95) plus CRC8 (crc8.h:57-67)
+ * per bitplane; the decoder side of the reference has no counterpart. */
+int dvc_ldpca_encode(dvc_ctx *ctx, int n, int count, const uint8_t *bits, uint8_t *acc, uint8_t *crc);
+
 /* Reference-shaped single-bitplane call: LdpcaDecoder(LR_intrinsic,
  * accumulatedSyndrome, decoded, &rate, crc, RateLowerBound) with the
  * accumulated syndrome as one bit per byte and the bound supplied by the

@@ -1,0 +1,76 @@
+"""dvcdec, the DvcDec-compatible executable: configuration handling on the CPU,
+golden sequences decoded through it on the GPU (RD report and decoded luma)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from dvc_b200 import build, synth
+
+CFG = """# decoder configuration (the reference decoder's keys)
+OriginalSequence  = "{d}/ori.yuv"
+WZBitstream       = "{d}/seq.wz"
+KeyFrameSequence  = "{d}/key.yuv"
+KeyFrameInfo      = "{d}/stat.txt"
+RDFile            = "{d}/rd"
+OutputSequences   = "{d}/dec"
+FrameRate         = 15
+ParallelMode      = 2
+UseCoreNum        = 1
+IntraBitstream    = "{d}/seq.intra"
+"""
+
+
+def _cli():
+    if not os.path.exists(build.CLI):
+        build.build()
+    return build.CLI
+
+
+def _setup(tmp_path, g):
+    d = str(tmp_path)
+    ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
+    synth.write_yuv420(os.path.join(d, "ori.yuv"), ori)
+    synth.write_yuv420(os.path.join(d, "key.yuv"), key)
+    synth.write_frame_stat(os.path.join(d, "stat.txt"), int(g["n_frames"]))
+    g["wz"].tofile(os.path.join(d, "seq.wz"))
+    open(os.path.join(d, "seq.intra"), "wb").close()
+    cfg = os.path.join(d, "decoder.cfg")
+    open(cfg, "w").write(CFG.format(d=d))
+    return d, cfg
+
+
+def test_cli_rejects_bad_arguments(tmp_path):
+    r = subprocess.run([_cli()], capture_output=True, text=True)
+    assert r.returncode != 0 and "Usage" in r.stderr
+    bad = tmp_path / "bad.cfg"
+    bad.write_text('NoSuchKey = "x"\n')
+    r = subprocess.run([_cli(), "-d", str(bad)], capture_output=True, text=True)
+    assert r.returncode != 0 and "not recognized" in r.stderr
+    short = tmp_path / "short.cfg"
+    short.write_text('WZBitstream = "x"\n')
+    r = subprocess.run([_cli(), "-d", str(short)], capture_output=True, text=True)
+    assert r.returncode != 0 and "Too few parameters" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seq", ["qcif_g4_q8", "cif_g2_q2"])
+def test_cli_decodes_golden_sequence(tmp_path, golden_dir, seq):
+    g = dict(np.load(os.path.join(golden_dir, f"seq_{seq}.npz")))
+    d, cfg = _setup(tmp_path, g)
+    r = subprocess.run([_cli(), "-d", cfg, "-GPUid=0"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    n = int(g["n_frames"])
+    h, w = g["dec_y"].shape[1:]
+    dec = np.fromfile(os.path.join(d, "dec.yuv"), np.uint8).reshape(n, h, w)
+    rd = open(os.path.join(d, "rd.txt")).read().splitlines()
+    for f, b, p, wz in zip(g["frames"], g["bits"], g["psnr"], g["is_wz"]):
+        f = int(f)
+        line = [x for x in rd if x.startswith("FrameNo: %d," % f)][0]
+        if wz:
+            assert np.array_equal(dec[f], g["dec_y"][f]), f"frame {f}"
+            assert "Bits: %d, PSNR: %.2f (WZ)" % (b, p) in line
+        else:
+            assert "(KY)" in line
+    assert any(x.startswith("Average WZ decoding speed:") for x in rd)
