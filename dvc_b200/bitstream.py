@@ -10,7 +10,8 @@ WZ bitstream (DvcDec/src/wzbitstream.cpp:129-210, readGOP :13-126):
         intraMode u8 [+ JBIG-coded 8x8 intra map],
         per bitplane: CRC-8 u8 + N/8 bytes of accumulated syndrome (MSB first).
 
-The JBIG mode maps are decoded by ``jbig.decode_mode_map`` when present.
+The JBIG mode maps are decoded by ``jbig.decode_mode_map`` (the library's T.82
+decoder).
 """
 import numpy as np
 

@@ -221,7 +221,6 @@ WzStream read_wz(const std::string &path) {
     return p;
   };
   const int n = s.w * s.h / 16, nb88 = s.w * s.h / 64;
-  (void)nb88;
   int qb = 0;
   for (int j = 0; j < 16; j++) qb += kQBits[s.q][j];
   std::vector<std::array<int, 3>> order;
@@ -249,10 +248,17 @@ WzStream read_wz(const std::string &path) {
     for (int k = 0; k < 2; k++) {
       const int flag = *take(1);
       (k == 0 ? fr.skip_mode : fr.intra_mode) = flag;
-      // the JBIG-coded 8x8 mode map that follows a set flag (wzbitstream.cpp:38-66)
-      // needs a JBIG decoder, which this build does not have
-      if (flag == 1)
-        die(std::string(k == 0 ? "SkipBlock" : "IntraMode") + " mode maps (JBIG) are not supported by this build");
+      if (flag == 1) {
+        // the JBIG-coded 8x8 mode map that follows a set flag (wzbitstream.cpp:38-66)
+        std::vector<uint8_t> map(nb88);
+        size_t used = 0;
+        if (dvc_jbig_decode_mode_map(&d[pos], d.size() - pos, s.w / 8, s.h / 8, map.data(), &used) != DVC_OK)
+          die("JBIG mode map of frame " + std::to_string(fr.idx) + " could not be decoded");
+        pos += used;
+        (k == 0 ? fr.skip_bits : fr.intra_bits) = (int)(used << 3) + 1;
+        for (int b = 0; b < nb88; b++)
+          if (map[b]) fr.mode[b] = (uint8_t)(k == 0 ? 2 : 1);
+      }
     }
     fr.crc.resize(qb);
     fr.acc.resize((size_t)qb * (n / 8));

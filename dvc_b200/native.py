@@ -93,6 +93,7 @@ FRAME_API = {
                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
     "dvc_ldpca_encode": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p],
+    "dvc_jbig_decode_mode_map": [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)],
 }
 
 

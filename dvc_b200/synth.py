@@ -11,6 +11,9 @@ value distributions of the benchmark configurations:
 * ``cif``: 352x288, sinusoid periods scaled x2 (8-80 px), four 48x48 objects.
 * ``cif_fast``: 352x288, global velocity in [-8, 8], six objects of 16-64 px
   moving at [-10, 10] px/frame.
+* ``qcif_still`` / ``cif_still``: as ``qcif`` / ``cif`` with a still background
+  (no global motion) and N(0, 1) noise, so that the encoder's skip test (8x8
+  block MSE against the past frame below 10) finds skip blocks.
 
 Chroma planes are constant 128 (4:2:0).  Key frames are the original frames plus
 N(0, 2) noise, rounded and clipped; the key-frame info file carries a fixed
@@ -19,7 +22,8 @@ DvcDec/src/frame.cpp:197-247).
 """
 import numpy as np
 
-SHAPES = {"qcif": (176, 144), "cif": (352, 288), "cif_fast": (352, 288)}
+SHAPES = {"qcif": (176, 144), "cif": (352, 288), "cif_fast": (352, 288), "qcif_still": (176, 144),
+          "cif_still": (352, 288)}
 
 
 def _params(kind):
@@ -29,6 +33,10 @@ def _params(kind):
         return dict(per=(8.0, 80.0), vel=3, n_obj=4, obj=(48, 48), ovel=4)
     if kind == "cif_fast":
         return dict(per=(8.0, 80.0), vel=8, n_obj=6, obj=(16, 64), ovel=10)
+    if kind == "qcif_still":
+        return dict(per=(4.0, 40.0), vel=0, n_obj=2, obj=(32, 32), ovel=4, noise=1.0)
+    if kind == "cif_still":
+        return dict(per=(8.0, 80.0), vel=0, n_obj=4, obj=(48, 48), ovel=4, noise=1.0)
     raise ValueError(kind)
 
 
@@ -70,7 +78,7 @@ def make_sequence(kind, n_frames, seed):
             x = (o["x"] + o["vx"] * t) % (w - s)
             y = (o["y"] + o["vy"] * t) % (h - s)
             f[y:y + s, x:x + s] = tex[o["sy"]:o["sy"] + s, o["sx"]:o["sx"] + s]
-        f = np.clip(np.rint(f + rng.normal(0.0, 3.0, f.shape)), 0, 255)
+        f = np.clip(np.rint(f + rng.normal(0.0, p.get("noise", 3.0), f.shape)), 0, 255)
         k = np.clip(np.rint(f + rng.normal(0.0, 2.0, f.shape)), 0, 255)
         orig[t] = f.astype(np.uint8)
         key[t] = k.astype(np.uint8)

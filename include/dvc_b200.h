@@ -59,6 +59,16 @@ const char *dvc_last_error(dvc_ctx *ctx);
 int dvc_ldpca_decode(dvc_ctx *ctx, int n, int count, const float *lr, const uint8_t *acc, const uint8_t *crc,
                      uint8_t *decoded, int *results, float *entropy, int max_iter);
 
+/* JBIG (T.82) decoder for a skip or intra mode map of the WZ bitstream: the
+ * coded stripe that follows a set skipMode / intraMode byte, decoded into
+ * map[h*w] (1 = the 8x8 block has the mode), with *used = the bytes it
+ * occupies (through the closing SDNORM/SDRST marker).  w x h = Block88Width x
+ * Block88Height (22x18 QCIF, 44x36 CIF).  Replaces the reference's
+ * simple_JBIG_dec over JBIG-KIT with the header it rebuilds
+ * (DvcDec/src/wzbitstream.cpp:38-66, sJBIG.cpp:49-104).  Host code, no GPU.
+ * DVC_E_DATA for a truncated stream or a stream with an adaptive-template move. */
+int dvc_jbig_decode_mode_map(const uint8_t *data, size_t len, int w, int h, uint8_t *map, size_t *used);
+
 /* LDPCA encoder on the device: for `count` source bitplanes of n bits
  * (bits[count*n], one 0/1 byte per bit) the accumulated syndromes acc[count*n/8]
  * (full-rate syndrome H*x, prefix-xored over the rows, packed MSB first as in

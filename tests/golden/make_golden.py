@@ -11,10 +11,16 @@ decoder computed:
                    code, rate, entropy) captured through oracle/ref_capture.cpp.
   ldpca_<n>.npz    LDPCA known-answer vectors: LR, accumulated syndrome bytes,
                    CRC, and the reference's entropy bound, rate, decoded bits.
+  jbig_maps.npz    mode maps coded by the reference's JBIG encoder, with the
+                   map its JBIG decoder returns and the bytes it consumes
+                   (oracle/_ref/libjbig{enc,dec}.so, oracle/jbig_ref.cpp).
+
+The *_skip sequences are encoded with SkipBlock 1 on still-camera content, so
+their WZ frames carry JBIG-coded skip maps.
 
 Usage (in the build container, after `make -C oracle ref` and
 `python oracle/ladder_dir.py oracle/_ref`):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]   # default: all
 """
 import os
 import sys
@@ -30,16 +36,18 @@ from dvc_b200 import synth  # noqa: E402
 from oracle import refrun  # noqa: E402
 import ladders as lad  # noqa: E402
 
-# name: (kind, frames, gop, qindex, seed)
+# name: (kind, frames, gop, qindex, seed[, skip])
 SEQUENCES = {
     "qcif_g2_q4": ("qcif", 5, 2, 4, 11),
     "qcif_g4_q8": ("qcif", 5, 4, 8, 12),
     "qcif_g2_q1": ("qcif", 3, 2, 1, 13),
     "cif_g2_q2": ("cif", 3, 2, 2, 21),
+    "qcif_still_g2_q4_skip": ("qcif_still", 5, 2, 4, 41, 1),
+    "cif_still_g4_q6_skip": ("cif_still", 5, 4, 6, 42, 1),
 }
 
 
-def run(name, kind, n_frames, gop, q, seed, tmp):
+def run(name, kind, n_frames, gop, q, seed, tmp, skip=0):
     w, h = synth.SHAPES[kind]
     size = "QCIF" if w == 176 else "CIF"
     ori, key = synth.make_sequence(kind, n_frames, seed)
@@ -49,7 +57,7 @@ def run(name, kind, n_frames, gop, q, seed, tmp):
     synth.write_yuv420(oy, ori)
     synth.write_yuv420(ky, key)
     synth.write_frame_stat(st, n_frames)
-    wz, intra, _ = refrun.encode(oy, ky, n_frames, size, gop, q)
+    wz, intra, _ = refrun.encode(oy, ky, n_frames, size, gop, q, skip=skip)
     cap = os.path.join(d, "cap.bin")
     r = refrun.decode(oy, wz, intra, ky, st, mode=0, capture=cap)
     dec_y = np.frombuffer(r["yuv"], np.uint8).reshape(-1, h, w)
@@ -70,7 +78,7 @@ def run(name, kind, n_frames, gop, q, seed, tmp):
     frames = sorted(rd)
     np.savez_compressed(
         os.path.join(HERE, f"seq_{name}.npz"),
-        kind=kind, n_frames=n_frames, gop=gop, qindex=q, seed=seed,
+        kind=kind, n_frames=n_frames, gop=gop, qindex=q, seed=seed, skip=skip,
         wz=np.frombuffer(open(wz, "rb").read(), np.uint8),
         dec_y=dec_y,
         frames=np.array(frames), bits=np.array([rd[f][0] for f in frames]),
@@ -100,11 +108,47 @@ def ldpca_fixture(recs, n, name, limit):
     )
 
 
+def jbig_fixture(count=240, seed=77):
+    """Random and blocky mode maps of both sizes through the reference's JBIG code."""
+    import ctypes as C
+    enc = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libjbigenc.so"))
+    dec = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libjbigdec.so"))
+    rng = np.random.default_rng(seed)
+    streams, maps, used, sizes = [], [], [], []
+    for t in range(count):
+        w, h = ((22, 18), (44, 36))[t % 2]
+        p = rng.uniform(0.0, 1.0)
+        if t % 3 == 0:
+            m = np.kron((rng.random(((h + 1) // 2, (w + 1) // 2)) < p).astype(np.uint8),
+                        np.ones((2, 2), np.uint8))[:h, :w]
+        else:
+            m = (rng.random((h, w)) < p).astype(np.uint8)
+        m = np.ascontiguousarray(m)
+        out = np.zeros(8192, np.uint8)
+        n = enc.jbigref_encode(m.ctypes.data_as(C.c_void_p), w, h, out.ctypes.data_as(C.c_void_p), 8192)
+        back = np.zeros((h, w), np.uint8)
+        u = dec.jbigref_decode(out.ctypes.data_as(C.c_void_p), n, w, h, back.ctypes.data_as(C.c_void_p))
+        assert np.array_equal(back, m) and u == n
+        streams.append(out[:n].copy())
+        maps.append(m.reshape(-1))
+        used.append(u)
+        sizes.append((w, h))
+    off = np.cumsum([0] + [len(x) for x in streams])
+    np.savez_compressed(os.path.join(HERE, "jbig_maps.npz"), data=np.concatenate(streams), offsets=off,
+                        maps=np.concatenate(maps), map_offsets=np.cumsum([0] + [len(x) for x in maps]),
+                        used=np.array(used), sizes=np.array(sizes))
+
+
 def main():
     import tempfile
     tmp = tempfile.mkdtemp(prefix="dvc_golden_")
+    want = set(sys.argv[1:])
+    if not want or "jbig_maps" in want:
+        jbig_fixture()
     for name, args in SEQUENCES.items():
-        recs, n = run(name, *args, tmp)
+        if want and name not in want:
+            continue
+        recs, n = run(name, *args[:5], tmp, *args[5:])
         print(name, "bitplanes", len(recs))
         if name == "qcif_g4_q8":
             ldpca_fixture(recs, n, "qcif", 48)
