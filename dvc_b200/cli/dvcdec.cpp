@@ -343,8 +343,6 @@ int main(int argc, char **argv) {
   printf("Read WZ bitstream file...\n");
   WzStream s = read_wz(o.value[1]);
   if (s.deblock) die("DeblockingFilter 1 streams are not supported by this build");
-  for (auto &kv : s.wz)
-    if (kv.second.intra_mode) die("IntraMode 1 streams (intra blocks) are not supported by this build");
   const size_t fs = (size_t)s.w * s.h;
   printf("Read original sequence...\n");
   auto ori = read_sequence(o.value[0], s.frames, s.w, s.h);
@@ -374,6 +372,44 @@ int main(int argc, char **argv) {
   };
   for (int i = start; i <= end; i += s.gop) rec(i, std::min(i + s.gop, end));
 
+  // intra blocks (IntraMode 1): one bitstream for the sequence, read frame by
+  // frame in decoding order, frames before startFrame included (skipGOP,
+  // DVC_Decoder.cpp:476-510); written over the key-frame content
+  std::map<int, int> intra_bits;
+  bool any_intra = false;
+  for (auto &kv : s.wz) any_intra = any_intra || kv.second.intra_mode;
+  if (any_intra) {
+    printf("Read Intra bitstream file...\n");
+    FILE *f = fopen(o.value[9].c_str(), "rb");
+    if (!f) die("File " + o.value[9] + " doesn't exist");
+    std::vector<uint8_t> ib;
+    uint8_t tmp[65536];
+    size_t r;
+    while ((r = fread(tmp, 1, sizeof tmp, f)) > 0) ib.insert(ib.end(), tmp, tmp + r);
+    fclose(f);
+    std::vector<int> order;
+    std::function<void(int, int)> walk = [&](int b, int e) {
+      const int m = (b + e) / 2;
+      if (m > b) {
+        order.push_back(m);
+        walk(b, m);
+        walk(m, e);
+      }
+    };
+    for (int i = 0; i < start; i += s.gop) walk(i, std::min(i + s.gop, end));
+    for (int i = start; i <= end; i += s.gop) walk(i, std::min(i + s.gop, end));
+    size_t bit = 0;
+    for (int m : order) {
+      const WzFrame &w = s.wz[m];
+      if (!w.intra_mode) continue;
+      const size_t before = bit;
+      if (dvc_intra_decode_frame(ib.data(), ib.size(), &bit, s.w, s.h, s.intra_qp, w.mode.data(), recon[m].data()) !=
+          DVC_OK)
+        die("intra bitstream of frame " + std::to_string(m) + " could not be decoded");
+      intra_bits[m] = (int)(bit - before);
+    }
+  }
+
   const std::string root = exe_dir() + "/..";
   dvc_ctx *ctx = nullptr;
   if (dvc_create((root + "/ladders").c_str(), (root + "/_tables").c_str(), o.gpu, &ctx) != DVC_OK)
@@ -382,7 +418,9 @@ int main(int argc, char **argv) {
   double device_ms = 0.0;
   std::vector<dvc_wz_frame> fr(todo.size());
   std::map<int, int> item_of;
-  std::vector<std::vector<uint8_t>> outbuf(todo.size(), std::vector<uint8_t>(fs, 0));
+  // each frame starts from its key-frame content with its intra blocks written in
+  std::vector<std::vector<uint8_t>> outbuf;
+  for (int m : todo) outbuf.push_back(recon[m]);
   for (size_t k = 0; k < todo.size(); k++) item_of[todo[k]] = (int)k;
   for (size_t k = 0; k < todo.size(); k++) {
     auto it = s.wz.find(todo[k]);
@@ -421,7 +459,7 @@ int main(int argc, char **argv) {
       if (dvc_session_frame(ses, (int)k, recon[todo[k]].data(), &wz_bits, nullptr) != DVC_OK)
         die(std::string("result read failed: ") + dvc_last_error(ctx));
       const WzFrame &w = s.wz[todo[k]];
-      bits[todo[k]] = w.skip_bits + w.intra_bits + wz_bits;
+      bits[todo[k]] = w.skip_bits + w.intra_bits + wz_bits + (intra_bits.count(todo[k]) ? intra_bits[todo[k]] : 0);
       psnr[todo[k]] = frame_psnr(recon[todo[k]].data(), ori[todo[k]].data(), fs);
       is_wz[todo[k]] = 1;
     }

@@ -1,0 +1,344 @@
+// Intra blocks of WZ frames (IntraMode 1): host decoder of the reference's
+// intra bitstream.
+//
+// The reference codes the 4x4 blocks of intra 8x8 blocks H.264-style
+// (DvcDec/src/intra.cpp:187-268, vlc.cpp:423-761): CAVLC coefficients
+// (coeff_token, trailing-one signs, levels with an adaptive suffix length,
+// total_zeros, run_before; the coeff_token table chosen by the predicted
+// number of non-zero coefficients of the left and upper intra blocks),
+// de-quantisation ROUND(c * 2^((QP-4)/6) * 64 pre-scale) in double, the 4x4
+// integer inverse transform with a final >> 6, and DC prediction from the
+// neighbouring pixels of left / upper blocks that are themselves intra.
+// The bitstream is one bit string for the whole sequence: every intra 4x4
+// block of every frame, frames in decoding order, blocks in raster order.
+//
+// The VLC tables are the standard's (ITU-T H.264 tables 9-5, 9-7 and 9-10,
+// luma 4x4); they are written here as code strings and turned into prefix
+// codes at first use, where they are checked to be prefix-free.
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dvc_b200.h"
+
+namespace {
+
+// coeff_token, 0 <= nC < 2, 2 <= nC < 4, 4 <= nC < 8: code of
+// (TrailingOnes t, TotalCoeff c) at [c][t] ("" where t > c)
+const char *kCoeffToken[3][17][4] = {
+    {{"1", "", "", ""},
+     {"000101", "01", "", ""},
+     {"00000111", "000100", "001", ""},
+     {"000000111", "00000110", "0000101", "00011"},
+     {"0000000111", "000000110", "00000101", "000011"},
+     {"00000000111", "0000000110", "000000101", "0000100"},
+     {"0000000001111", "00000000110", "0000000101", "00000100"},
+     {"0000000001011", "0000000001110", "00000000101", "000000100"},
+     {"0000000001000", "0000000001010", "0000000001101", "0000000100"},
+     {"00000000001111", "00000000001110", "0000000001001", "00000000100"},
+     {"00000000001011", "00000000001010", "00000000001101", "0000000001100"},
+     {"000000000001111", "000000000001110", "00000000001001", "00000000001100"},
+     {"000000000001011", "000000000001010", "000000000001101", "00000000001000"},
+     {"0000000000001111", "000000000000001", "000000000001001", "000000000001100"},
+     {"0000000000001011", "0000000000001110", "0000000000001101", "000000000001000"},
+     {"0000000000000111", "0000000000001010", "0000000000001001", "0000000000001100"},
+     {"0000000000000100", "0000000000000110", "0000000000000101", "0000000000001000"}},
+    {{"11", "", "", ""},
+     {"001011", "10", "", ""},
+     {"000111", "00111", "011", ""},
+     {"0000111", "001010", "001001", "0101"},
+     {"00000111", "000110", "000101", "0100"},
+     {"00000100", "0000110", "0000101", "00110"},
+     {"000000111", "00000110", "00000101", "001000"},
+     {"00000001111", "000000110", "000000101", "000100"},
+     {"00000001011", "00000001110", "00000001101", "0000100"},
+     {"000000001111", "00000001010", "00000001001", "000000100"},
+     {"000000001011", "000000001110", "000000001101", "00000001100"},
+     {"000000001000", "000000001010", "000000001001", "00000001000"},
+     {"0000000001111", "0000000001110", "0000000001101", "000000001100"},
+     {"0000000001011", "0000000001010", "0000000001001", "0000000001100"},
+     {"0000000000111", "00000000001011", "0000000000110", "0000000001000"},
+     {"00000000001001", "00000000001000", "00000000001010", "0000000000001"},
+     {"00000000000111", "00000000000110", "00000000000101", "00000000000100"}},
+    {{"1111", "", "", ""},
+     {"001111", "1110", "", ""},
+     {"001011", "01111", "1101", ""},
+     {"001000", "01100", "01110", "1100"},
+     {"0001111", "01010", "01011", "1011"},
+     {"0001011", "01000", "01001", "1010"},
+     {"0001001", "001110", "001101", "1001"},
+     {"0001000", "001010", "001001", "1000"},
+     {"00001111", "0001110", "0001101", "01101"},
+     {"00001011", "00001110", "0001010", "001100"},
+     {"000001111", "00001010", "00001101", "0001100"},
+     {"000001011", "000001110", "00001001", "00001100"},
+     {"000001000", "000001010", "000001101", "00001000"},
+     {"0000001101", "000000111", "000001001", "000001100"},
+     {"0000001001", "0000001100", "0000001011", "0000001010"},
+     {"0000000101", "0000001000", "0000000111", "0000000110"},
+     {"0000000001", "0000000100", "0000000011", "0000000010"}}};
+
+// total_zeros for TotalCoeff 1..15 (index tc-1), value = position in the list
+const char *kTotalZeros[15][16] = {
+    {"1", "011", "010", "0011", "0010", "00011", "00010", "000011", "000010", "0000011", "0000010", "00000011",
+     "00000010", "000000011", "000000010", "000000001"},
+    {"111", "110", "101", "100", "011", "0101", "0100", "0011", "0010", "00011", "00010", "000011", "000010", "000001",
+     "000000"},
+    {"0101", "111", "110", "101", "0100", "0011", "100", "011", "0010", "00011", "00010", "000001", "00001", "000000"},
+    {"00011", "111", "0101", "0100", "110", "101", "100", "0011", "011", "0010", "00010", "00001", "00000"},
+    {"0101", "0100", "0011", "111", "110", "101", "100", "011", "0010", "00001", "0001", "00000"},
+    {"000001", "00001", "111", "110", "101", "100", "011", "010", "0001", "001", "000000"},
+    {"000001", "00001", "101", "100", "011", "11", "010", "0001", "001", "000000"},
+    {"000001", "0001", "00001", "011", "11", "10", "010", "001", "000000"},
+    {"000001", "000000", "0001", "11", "10", "001", "01", "00001"},
+    {"00001", "00000", "001", "11", "10", "01", "0001"},
+    {"0000", "0001", "001", "010", "1", "011"},
+    {"0000", "0001", "01", "1", "001"},
+    {"000", "001", "1", "01"},
+    {"00", "01", "1"},
+    {"0", "1"}};
+
+// run_before for zerosLeft 1..6 and > 6 (index min(zerosLeft, 7) - 1)
+const char *kRunBefore[7][15] = {{"1", "0"},
+                                 {"1", "01", "00"},
+                                 {"11", "10", "01", "00"},
+                                 {"11", "10", "01", "001", "000"},
+                                 {"11", "10", "011", "010", "001", "000"},
+                                 {"11", "000", "001", "011", "010", "101", "100"},
+                                 {"111", "110", "101", "100", "011", "010", "001", "0001", "00001", "000001",
+                                  "0000001", "00000001", "000000001", "0000000001", "00000000001"}};
+
+// zig-zag scan (DvcDec/src/global.cpp:36-41)
+const int kZigzag[16] = {0, 1, 4, 8, 5, 2, 3, 6, 9, 12, 13, 10, 7, 11, 14, 15};
+
+struct Code {
+  int len;
+  uint32_t bits;
+  int sym;
+};
+using Table = std::vector<Code>;
+
+struct Tables {
+  Table coeff[3], total_zeros[15], run_before[7];
+  bool ok = true;
+};
+
+void add(Table &t, const char *s, int sym) {
+  if (!s || !*s) return;
+  Code c{(int)strlen(s), 0u, sym};
+  for (const char *p = s; *p; p++) c.bits = (c.bits << 1) | (uint32_t)(*p == '1');
+  t.push_back(c);
+}
+
+bool prefix_free(const Table &t) {
+  for (size_t i = 0; i < t.size(); i++)
+    for (size_t j = 0; j < t.size(); j++) {
+      if (i == j || t[i].len > t[j].len) continue;
+      if ((t[j].bits >> (t[j].len - t[i].len)) == t[i].bits) return false;
+    }
+  return true;
+}
+
+const Tables &tables() {
+  static Tables T;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    for (int v = 0; v < 3; v++) {
+      for (int c = 0; c <= 16; c++)
+        for (int t = 0; t < 4; t++) add(T.coeff[v], kCoeffToken[v][c][t], c * 4 + t);
+      T.ok = T.ok && prefix_free(T.coeff[v]);
+    }
+    for (int i = 0; i < 15; i++) {
+      for (int z = 0; z < 16; z++) add(T.total_zeros[i], kTotalZeros[i][z], z);
+      T.ok = T.ok && prefix_free(T.total_zeros[i]);
+    }
+    for (int i = 0; i < 7; i++) {
+      for (int r = 0; r < 15; r++) add(T.run_before[i], kRunBefore[i][r], r);
+      T.ok = T.ok && prefix_free(T.run_before[i]);
+    }
+  });
+  return T;
+}
+
+struct Bits {
+  const uint8_t *d;
+  size_t nbits, pos;
+  bool bad = false;
+  int bit() {
+    if (pos >= nbits) {
+      bad = true;
+      return 0;
+    }
+    const int b = (d[pos >> 3] >> (7 - (pos & 7))) & 1;
+    pos++;
+    return b;
+  }
+  uint32_t read(int n) {
+    uint32_t v = 0;
+    for (int i = 0; i < n; i++) v = (v << 1) | (uint32_t)bit();
+    return v;
+  }
+  int vlc(const Table &t) {
+    uint32_t v = 0;
+    for (int len = 1; len <= 16; len++) {
+      v = (v << 1) | (uint32_t)bit();
+      if (bad) return -1;
+      for (const Code &c : t)
+        if (c.len == len && c.bits == v) return c.sym;
+    }
+    bad = true;
+    return -1;
+  }
+};
+
+struct Frame {
+  int w, h, b4w, b4h, b8w;
+  const uint8_t *mode;  // 8x8 block modes
+  bool intra(int bx, int by) const { return mode[(by >> 1) * b8w + (bx >> 1)] == 1; }
+};
+
+// levels of one block in scan order into coeff (zig-zag positions); returns
+// the total coefficient count, -1 on a bitstream error
+int read_coeffs(Bits &bs, const Frame &F, int bx, int by, std::vector<int> &nnz, int coeff[16]) {
+  const Tables &T = tables();
+  int nc = 0, cnt = 0;
+  if (bx > 0 && F.intra(bx - 1, by)) {
+    nc += nnz[by * F.b4w + bx - 1];
+    cnt++;
+  }
+  if (by > 0 && F.intra(bx, by - 1)) {
+    nc += nnz[(by - 1) * F.b4w + bx];
+    cnt++;
+  }
+  if (cnt == 2) nc = (nc + 1) >> 1;
+  int total, t1;
+  if (nc >= 8) {  // 6-bit fixed-length coeff_token
+    const uint32_t v = bs.read(6);
+    if (v == 3) {
+      total = 0;
+      t1 = 0;
+    } else {
+      total = (int)(v >> 2) + 1;
+      t1 = (int)(v & 3);
+      if (t1 > total) return -1;
+    }
+  } else {
+    const int sym = bs.vlc(T.coeff[nc < 2 ? 0 : nc < 4 ? 1 : 2]);
+    if (sym < 0) return -1;
+    total = sym >> 2;
+    t1 = sym & 3;
+  }
+  nnz[by * F.b4w + bx] = total;
+  memset(coeff, 0, 16 * sizeof(int));
+  if (total == 0) return 0;
+  int level[16] = {0}, run[16] = {0};
+  // trailing ones, highest frequency first
+  for (int k = total - 1; k >= total - t1; k--) level[k] = bs.bit() ? -1 : 1;
+  int suffix_len = (total > 10 && t1 < 3) ? 1 : 0;
+  for (int k = total - 1 - t1; k >= 0; k--) {
+    int prefix = 0;
+    while (!bs.bit()) {
+      if (bs.bad || ++prefix > 15) return -1;
+    }
+    int code = (std::min(15, prefix) << suffix_len);
+    const int ssize = (prefix == 14 && suffix_len == 0) ? 4 : (prefix >= 15 ? prefix - 3 : suffix_len);
+    if (ssize > 0) code += (int)bs.read(ssize);
+    if (prefix >= 15 && suffix_len == 0) code += 15;
+    if (k == total - 1 - t1 && t1 < 3) code += 2;
+    const int v = (code % 2 == 0) ? (code + 2) >> 1 : (-code - 1) >> 1;
+    level[k] = v;
+    if (suffix_len == 0) suffix_len = 1;
+    const int a = v < 0 ? -v : v;
+    if (a > (3 << (suffix_len - 1)) && suffix_len < 6) suffix_len++;
+    if (k == total - 1 - t1 && a > 3) suffix_len = 2;
+  }
+  int zeros = 0;
+  if (total < 16) {
+    zeros = bs.vlc(T.total_zeros[total - 1]);
+    if (zeros < 0) return -1;
+  }
+  int left = zeros, i = total - 1;
+  while (left > 0 && i > 0) {
+    const int r = bs.vlc(T.run_before[std::min(left, 7) - 1]);
+    if (r < 0 || r > left) return -1;
+    run[i] = r;
+    left -= r;
+    i--;
+  }
+  run[i] = left;
+  int pos = 0;
+  for (int k = 0; k < total; k++) {
+    pos += run[k];
+    if (pos > 15) return -1;
+    coeff[kZigzag[pos]] = level[k];
+    pos++;
+  }
+  return bs.bad ? -1 : total;
+}
+
+// H.264 4x4 inverse transform with the final division by 64 (intra.cpp:35-77)
+void inverse44(int *b) {
+  int t[16];
+  for (int c = 0; c < 4; c++) {
+    const int x0 = b[c], x1 = b[4 + c], x2 = b[8 + c], x3 = b[12 + c];
+    t[c] = x0 + x1 + x2 + (x3 >> 1);
+    t[4 + c] = x0 + (x1 >> 1) - x2 - x3;
+    t[8 + c] = x0 - (x1 >> 1) - x2 + x3;
+    t[12 + c] = x0 - x1 + x2 - (x3 >> 1);
+  }
+  for (int r = 0; r < 4; r++) {
+    const int y0 = t[4 * r], y1 = t[4 * r + 1], y2 = t[4 * r + 2], y3 = t[4 * r + 3];
+    b[4 * r] = y0 + y1 + y2 + (y3 >> 1);
+    b[4 * r + 1] = y0 + (y1 >> 1) - y2 - y3;
+    b[4 * r + 2] = y0 - (y1 >> 1) - y2 + y3;
+    b[4 * r + 3] = y0 - y1 + y2 - (y3 >> 1);
+  }
+  for (int i = 0; i < 16; i++) b[i] >>= 6;
+}
+
+int round_half_away(double x) { return x >= 0.0 ? (int)(x + 0.5) : -(int)(-x + 0.5); }  // defines.h:23
+
+}  // namespace
+
+extern "C" int dvc_intra_decode_frame(const uint8_t *stream, size_t stream_bytes, size_t *bit_offset, int width,
+                                      int height, int intra_qp, const uint8_t *mode, uint8_t *recon) {
+  if (!stream || !bit_offset || !mode || !recon || !((width == 176 && height == 144) || (width == 352 && height == 288)) ||
+      intra_qp < 0 || intra_qp > 51)
+    return DVC_E_ARG;
+  if (!tables().ok) return DVC_E_DATA;
+  Frame F{width, height, width / 4, height / 4, width / 8, mode};
+  Bits bs{stream, stream_bytes * 8, *bit_offset};
+  // de-quantisation scale: Qstep * 64 * pre-scale (intra.cpp:214, transform.cpp:12-52)
+  const double qstep = pow(2.0, ((double)intra_qp - 4.0) / 6.0);
+  const double a2 = 0.25, b2 = 0.4, ab = 0.5 * sqrt(0.4);
+  const double pre[16] = {a2, ab, a2, ab, ab, b2, ab, b2, a2, ab, a2, ab, ab, b2, ab, b2};
+  std::vector<int> nnz((size_t)F.b4w * F.b4h, 0);
+  for (int by = 0; by < F.b4h; by++)
+    for (int bx = 0; bx < F.b4w; bx++) {
+      if (!F.intra(bx, by)) continue;
+      int coeff[16], blk[16];
+      if (read_coeffs(bs, F, bx, by, nnz, coeff) < 0) return DVC_E_DATA;
+      for (int i = 0; i < 16; i++) blk[i] = round_half_away((double)coeff[i] * qstep * (pre[i] * 64.0));
+      // DC prediction from intra neighbours (intra.cpp:120-184)
+      const int top = by * 4, left = bx * 4;
+      const bool up = by > 0 && F.intra(bx, by - 1), lf = bx > 0 && F.intra(bx - 1, by);
+      int s = 0;
+      if (up)
+        for (int j = 0; j < 4; j++) s += recon[(top - 1) * width + left + j];
+      if (lf)
+        for (int i = 0; i < 4; i++) s += recon[(top + i) * width + left - 1];
+      const int pred = (up && lf) ? (s + 4) >> 3 : (up || lf) ? (s + 2) >> 2 : 128;
+      inverse44(blk);
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+          const int v = blk[4 * i + j] + pred;
+          recon[(top + i) * width + left + j] = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
+        }
+    }
+  *bit_offset = bs.pos;
+  return DVC_OK;
+}

@@ -1023,7 +1023,10 @@ cudaError_t launch_frame_prep(FrameDev *fr, int nf, int w, int h, cudaStream_t s
   return cudaGetLastError();
 }
 
+// A batch whose frames have no WZ block (every block intra or skipped) has
+// max_nsir == 0: the per-WZ-block kernels have nothing to do and are not launched.
 cudaError_t launch_noise_dist(FrameDev *fr, int nf, int max_nsir, const XlmDev &xt, int band, cudaStream_t s) {
+  if (max_nsir <= 0) return cudaSuccess;
   noise_dist_kernel<256><<<dim3(max_nsir, nf), 256, 0, s>>>(fr, xt, band);
   return cudaGetLastError();
 }
@@ -1035,6 +1038,7 @@ cudaError_t launch_cond_bit(FrameDev *fr, int nf, int w, int h, int band, int bi
 
 cudaError_t launch_band_end(FrameDev *fr, int nf, int w, int h, int max_nsir, int band, const XlmDev &xt,
                             cudaStream_t s) {
+  if (max_nsir <= 0) return cudaSuccess;
   recon_kernel<<<g2(max_nsir, 128, nf), 128, 0, s>>>(fr, band);
   update_si_kernel<128><<<dim3(max_nsir, nf), 128, 0, s>>>(fr, band);
   over_complete_kernel<<<dim3((w - 3 + 127) / 128, nf, h - 3), 128, 0, s>>>(fr, band);
@@ -1044,6 +1048,7 @@ cudaError_t launch_band_end(FrameDev *fr, int nf, int w, int h, int max_nsir, in
 }
 
 cudaError_t launch_final_inverse(FrameDev *fr, int nf, int max_nsir, cudaStream_t s) {
+  if (max_nsir <= 0) return cudaSuccess;
   recon_kernel<<<g2(max_nsir, 128, nf), 128, 0, s>>>(fr, -1);
   return cudaGetLastError();
 }

@@ -44,29 +44,36 @@ def decode_levels(stream, start=0, end=None):
     return levels
 
 
-def decode_sequence(ctx, stream, key_frames, ori_frames=None, key_bits=None, key_psnr=None, intra=None):
+def decode_sequence(ctx, stream, key_frames, ori_frames=None, key_bits=None, key_psnr=None, intra_bitstream=None):
     """Decode every WZ frame. Returns dict(recon, bits, psnr, planes, deblock_flag).
 
-    intra: optional callable(frame_index, mode) -> uint8 HxW with intra-block pixels.
+    intra_bitstream: bytes of the sequence's intra bitstream, needed when frames
+    have intra blocks (IntraMode 1); their pixels are decoded first
+    (dvc_b200.intra) and the frame's intra bits count into its rate
+    (DVC_Decoder.cpp:42-46).
     """
     recon = np.array(key_frames, np.uint8, copy=True)
     bits = dict(key_bits or {})
     ps = dict(key_psnr or {})
     planes, dbf = {}, {}
+    intra_px = {}
+    if any(fr.intra_mode for fr in stream.frames.values()):
+        if intra_bitstream is None:
+            raise ValueError("the stream has intra blocks; pass its intra bitstream")
+        from . import intra
+        intra_px = intra.decode_all(stream, intra_bitstream, recon)
     for lvl in decode_levels(stream):
         items = []
         for (m, b, e) in lvl:
             fr = stream.frames[m]
-            if fr.intra_mode:
-                if intra is None:
-                    raise NotImplementedError("frame %d has intra blocks; pass an intra decoder" % m)
-                recon[m] = intra(m, fr.mode)
+            if m in intra_px:
+                recon[m] = intra_px[m][0]
             items.append(frame_item(stream, fr, recon))
         outs = ctx.decode_wz_frames(items)
         for (m, b, e), o in zip(lvl, outs):
             fr = stream.frames[m]
             recon[m] = o["recon"]
-            bits[m] = fr.skip_bits + fr.intra_map_bits + o["wz_bits"]
+            bits[m] = fr.skip_bits + fr.intra_map_bits + o["wz_bits"] + (intra_px[m][1] if m in intra_px else 0)
             planes[m] = o["planes"]
             dbf[m] = o["deblock_flag"]
             if ori_frames is not None:

@@ -69,6 +69,18 @@ int dvc_ldpca_decode(dvc_ctx *ctx, int n, int count, const float *lr, const uint
  * DVC_E_DATA for a truncated stream or a stream with an adaptive-template move. */
 int dvc_jbig_decode_mode_map(const uint8_t *data, size_t len, int w, int h, uint8_t *map, size_t *used);
 
+/* Intra blocks of one WZ frame (IntraMode 1), decoded from the sequence's
+ * intra bitstream: CAVLC coefficients, de-quantisation with IntraQP, 4x4
+ * inverse transform, DC prediction from intra neighbours; the pixels of every
+ * 4x4 block inside an intra 8x8 block (mode[w*h/64] == 1) are written into
+ * recon[w*h], other pixels are left alone.  *bit_offset is the position in
+ * the bitstream, advanced past this frame's blocks (frames are read in the
+ * reference's decoding order).  Replaces intraRecon (DvcDec/src/intra.cpp:
+ * 187-268) with readCoeff4x4_CAVLC (vlc.cpp:613-761).  Host code, no GPU.
+ * DVC_E_DATA on a malformed or exhausted bitstream. */
+int dvc_intra_decode_frame(const uint8_t *stream, size_t stream_bytes, size_t *bit_offset, int width, int height,
+                           int intra_qp, const uint8_t *mode, uint8_t *recon);
+
 /* LDPCA encoder on the device: for `count` source bitplanes of n bits
  * (bits[count*n], one 0/1 byte per bit) the accumulated syndromes acc[count*n/8]
  * (full-rate syndrome H*x, prefix-xored over the rows, packed MSB first as in

@@ -16,7 +16,9 @@ decoder computed:
                    (oracle/_ref/libjbig{enc,dec}.so, oracle/jbig_ref.cpp).
 
 The *_skip sequences are encoded with SkipBlock 1 on still-camera content, so
-their WZ frames carry JBIG-coded skip maps.
+their WZ frames carry JBIG-coded skip maps; the *_intra sequences with
+SkipBlock 1 and IntraMode 1, so they also carry intra maps and an intra
+bitstream (stored as ``intra``).
 
 Usage (in the build container, after `make -C oracle ref` and
 `python oracle/ladder_dir.py oracle/_ref`):
@@ -36,7 +38,7 @@ from dvc_b200 import synth  # noqa: E402
 from oracle import refrun  # noqa: E402
 import ladders as lad  # noqa: E402
 
-# name: (kind, frames, gop, qindex, seed[, skip])
+# name: (kind, frames, gop, qindex, seed[, skip[, intra]])
 SEQUENCES = {
     "qcif_g2_q4": ("qcif", 5, 2, 4, 11),
     "qcif_g4_q8": ("qcif", 5, 4, 8, 12),
@@ -44,10 +46,13 @@ SEQUENCES = {
     "cif_g2_q2": ("cif", 3, 2, 2, 21),
     "qcif_still_g2_q4_skip": ("qcif_still", 5, 2, 4, 41, 1),
     "cif_still_g4_q6_skip": ("cif_still", 5, 4, 6, 42, 1),
+    "qcif_g2_q4_intra": ("qcif", 5, 2, 4, 11, 1, 1),
+    "cif_g4_q6_intra": ("cif", 5, 4, 6, 21, 1, 1),
+    "qcif_g4_q8_allintra": ("qcif", 5, 4, 8, 12, 1, 1),
 }
 
 
-def run(name, kind, n_frames, gop, q, seed, tmp, skip=0):
+def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0):
     w, h = synth.SHAPES[kind]
     size = "QCIF" if w == 176 else "CIF"
     ori, key = synth.make_sequence(kind, n_frames, seed)
@@ -57,9 +62,9 @@ def run(name, kind, n_frames, gop, q, seed, tmp, skip=0):
     synth.write_yuv420(oy, ori)
     synth.write_yuv420(ky, key)
     synth.write_frame_stat(st, n_frames)
-    wz, intra, _ = refrun.encode(oy, ky, n_frames, size, gop, q, skip=skip)
+    wz, intra_bs, _ = refrun.encode(oy, ky, n_frames, size, gop, q, skip=skip, intra=intra)
     cap = os.path.join(d, "cap.bin")
-    r = refrun.decode(oy, wz, intra, ky, st, mode=0, capture=cap)
+    r = refrun.decode(oy, wz, intra_bs, ky, st, mode=0, capture=cap)
     dec_y = np.frombuffer(r["yuv"], np.uint8).reshape(-1, h, w)
     rd = refrun.parse_rd(r["rd"])
     caps = refrun.read_capture(cap)
@@ -80,6 +85,7 @@ def run(name, kind, n_frames, gop, q, seed, tmp, skip=0):
         os.path.join(HERE, f"seq_{name}.npz"),
         kind=kind, n_frames=n_frames, gop=gop, qindex=q, seed=seed, skip=skip,
         wz=np.frombuffer(open(wz, "rb").read(), np.uint8),
+        intra=np.frombuffer(open(intra_bs, "rb").read(), np.uint8),
         dec_y=dec_y,
         frames=np.array(frames), bits=np.array([rd[f][0] for f in frames]),
         psnr=np.array([rd[f][1] for f in frames]),

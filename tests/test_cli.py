@@ -35,7 +35,10 @@ def _setup(tmp_path, g):
     synth.write_yuv420(os.path.join(d, "key.yuv"), key)
     synth.write_frame_stat(os.path.join(d, "stat.txt"), int(g["n_frames"]))
     g["wz"].tofile(os.path.join(d, "seq.wz"))
-    open(os.path.join(d, "seq.intra"), "wb").close()
+    if "intra" in g:
+        g["intra"].tofile(os.path.join(d, "seq.intra"))
+    else:
+        open(os.path.join(d, "seq.intra"), "wb").close()
     cfg = os.path.join(d, "decoder.cfg")
     open(cfg, "w").write(CFG.format(d=d))
     return d, cfg
@@ -55,7 +58,7 @@ def test_cli_rejects_bad_arguments(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("seq", ["qcif_g4_q8", "cif_g2_q2", "qcif_still_g2_q4_skip"])
+@pytest.mark.parametrize("seq", ["qcif_g4_q8", "cif_g2_q2", "qcif_still_g2_q4_skip", "cif_g4_q6_intra"])
 def test_cli_decodes_golden_sequence(tmp_path, golden_dir, seq):
     g = dict(np.load(os.path.join(golden_dir, f"seq_{seq}.npz")))
     d, cfg = _setup(tmp_path, g)

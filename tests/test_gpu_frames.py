@@ -11,12 +11,14 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("seq", ["qcif_g2_q4", "qcif_g4_q8", "qcif_g2_q1", "cif_g2_q2", "qcif_still_g2_q4_skip",
-                                 "cif_still_g4_q6_skip"])
+                                 "cif_still_g4_q6_skip", "qcif_g2_q4_intra", "cif_g4_q6_intra",
+                                 "qcif_g4_q8_allintra"])
 def test_sequence_matches_reference(gpu_ctx, golden_dir, seq):
     g = np.load(os.path.join(golden_dir, f"seq_{seq}.npz"))
     ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
     st = bs.parse_wz(g["wz"].tobytes())
-    res = decoder.decode_sequence(gpu_ctx, st, key, ori)
+    intra_bs = g["intra"].tobytes() if "intra" in g.files else None
+    res = decoder.decode_sequence(gpu_ctx, st, key, ori, intra_bitstream=intra_bs)
     for f, b, p, wz in zip(g["frames"], g["bits"], g["psnr"], g["is_wz"]):
         if wz:
             f = int(f)
