@@ -17,7 +17,8 @@
 // Every WZ frame of the requested range is decoded on the GPU in one
 // device-resident session: the GOP recursion (DVC_Decoder.cpp:26-474) becomes
 // levels of frames whose references are earlier levels' outputs.
-// ParallelMode and UseCoreNum are read and ignored.  The per-frame
+// Skip and intra maps, intra blocks and the deblocking filter are handled as
+// the reference does.  ParallelMode and UseCoreNum are read and ignored.  The per-frame
 // "Decoding time" of the RD report is the session's device time divided by
 // the number of WZ frames (the frames decode concurrently).
 #include <math.h>
@@ -342,7 +343,6 @@ int main(int argc, char **argv) {
 
   printf("Read WZ bitstream file...\n");
   WzStream s = read_wz(o.value[1]);
-  if (s.deblock) die("DeblockingFilter 1 streams are not supported by this build");
   const size_t fs = (size_t)s.w * s.h;
   printf("Read original sequence...\n");
   auto ori = read_sequence(o.value[0], s.frames, s.w, s.h);
@@ -448,6 +448,10 @@ int main(int argc, char **argv) {
     f.crc = w.crc.data();
     f.acc_synd = w.acc.data();
     f.recon = outbuf[k].data();
+    f.deblock = s.deblock;
+    f.intra_qp = s.intra_qp;
+    auto pw = s.wz.find(w.past);
+    f.past_mode = pw != s.wz.end() ? pw->second.mode.data() : nullptr;
   }
   if (!todo.empty()) {
     dvc_session *ses = nullptr;

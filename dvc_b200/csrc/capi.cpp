@@ -270,6 +270,9 @@ static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t 
     S.mode = f.mode;
     S.skip_mode = f.skip_mode;
     S.intra_mode = f.intra_mode;
+    S.deblock = f.deblock;
+    S.intra_qp = f.intra_qp;
+    S.past_mode = f.past_mode;
     for (int j = 0; j < 16; j++) S.ac_range[j] = f.ac_range[j];
     S.crc = f.crc;
     S.acc = f.acc_synd;
@@ -523,6 +526,9 @@ extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *f
       sp.mode = f.mode;
       sp.skip_mode = f.skip_mode;
       sp.intra_mode = f.intra_mode;
+      sp.deblock = f.deblock;
+      sp.intra_qp = f.intra_qp;
+      sp.past_mode = f.past_mode;
       for (int j = 0; j < 16; j++) sp.ac_range[j] = f.ac_range[j];
       sp.crc = f.crc;
       sp.acc = f.acc_synd;

@@ -58,6 +58,7 @@ cudaError_t launch_cond_bit(FrameDev *fr, int nf, int w, int h, int band, int bi
 cudaError_t launch_band_end(FrameDev *fr, int nf, int w, int h, int max_nsir, int band, const XlmDev &xt,
                             cudaStream_t s);
 cudaError_t launch_final_inverse(FrameDev *fr, int nf, int max_nsir, cudaStream_t s);
+cudaError_t launch_deblock(FrameDev *fr, int nf, int w, int h, cudaStream_t s);
 
 static bool g_scales_done = false;
 
@@ -84,7 +85,7 @@ bool Slot::ensure(int w_, int h_, size_t pdf_floats, size_t in_bytes, size_t out
             smf.ensure(n * 81 * 4) && pdf.ensure(pdf_floats * 4) && mb_mv.ensure(b16n * sizeof(MVd)) &&
             fmv.ensure(b16n * sizeof(MVd)) && blk_mv.ensure(b8n * sizeof(MVd)) && blk_mv2.ensure(b8n * sizeof(MVd)) &&
             holes.ensure(b16n * 16) && mse.ensure(b8n * 8) && stats.ensure(32 * 4) && in.ensure(in_bytes) &&
-            out.ensure(out_bytes);
+            out.ensure(out_bytes) && db_img.ensure(fs) && db_mode.ensure(2 * n) && db_bs.ensure(2 * n * 8);
   w = w_;
   h = h_;
   return ok;
@@ -92,7 +93,7 @@ bool Slot::ensure(int w_, int h_, size_t pdf_floats, size_t in_bytes, size_t out
 
 void Slot::release() {
   DevBuf *all[] = {&si, &dbf, &residue, &side_trans, &recons_trans, &alpha, &lr, &oct, &smf, &pdf,
-                   &mb_mv, &fmv, &blk_mv, &blk_mv2, &holes, &mse, &stats, &in, &out};
+                   &mb_mv, &fmv, &blk_mv, &blk_mv2, &holes, &mse, &stats, &in, &out, &db_img, &db_mode, &db_bs};
   for (DevBuf *b : all) b->release();
 }
 
@@ -143,7 +144,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
   std::vector<std::vector<int>> plane_base(nf);
   int max_nsir = 0;
   struct Packed {
-    size_t mode, sir, sob, crc, acc, total;
+    size_t mode, sir, sob, crc, acc, pmode, total;
   };
   std::vector<Packed> pk(nf);
   std::vector<int> qb(nf);
@@ -157,7 +158,8 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     p.sob = align16(p.sir + (size_t)n * 4);
     p.crc = align16(p.sob + (size_t)n * 4);
     p.acc = align16(p.crc + (size_t)qb[f]);
-    p.total = align16(p.acc + (size_t)qb[f] * nb);
+    p.pmode = align16(p.acc + (size_t)qb[f] * nb);
+    p.total = align16(p.pmode + b8n);
     pinned_need += p.total;
   }
   const size_t fd_off = pinned_need;
@@ -250,6 +252,10 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     D.nsir = nsir;
     max_nsir = std::max(max_nsir, nsir);
     memcpy(P + p.crc, F.crc, qb[f]);
+    if (F.past_mode)
+      memcpy(P + p.pmode, F.past_mode, b8n);
+    else
+      memset(P + p.pmode, 0, b8n);
     memcpy(P + p.acc, F.acc, (size_t)qb[f] * nb);
     Slot &S = slots_[f];
     if (!S.ensure(w, h, (size_t)std::max(nsir, 1) * pdf_stride, p.total, (size_t)qb[f] * 20 + 64))
@@ -283,6 +289,14 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     D.mse = S.mse.as<double>();
     D.band_mean = S.stats.as<float>();
     D.band_var = S.stats.as<float>() + 16;
+    D.deblock = F.deblock ? 1 : 0;
+    D.db_qp = std::min(51, std::max(0, F.intra_qp));
+    D.db_pow = pow(2, (double)D.db_qp / 6.0);  // deblock.cpp:174, with the host's C library
+    D.past_is_wz = F.past_mode != nullptr;
+    D.past_mode = in + p.pmode;
+    D.db_img = S.db_img.as<uint8_t>();
+    D.db_mode = S.db_mode.as<uint8_t>();
+    D.db_bs = S.db_bs.as<double>();
     // bitplane index of each (band, bit) in this frame's bitstream order
     plane_base[f].assign(16, 0);
     int acc_planes = 0;
@@ -421,6 +435,9 @@ bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileSt
     if (!ctx.cuda_ok(launch_band_end(fdev, nf, w, h, max_nsir, band, ctx.xlm, s), "band reconstruction")) return false;
   }
   if (!ctx.cuda_ok(launch_final_inverse(fdev, nf, max_nsir, s), "inverse transform")) return false;
+  bool any_deblock = false;
+  for (int f = 0; f < nf; f++) any_deblock = any_deblock || fd[f].deblock;
+  if (any_deblock && !ctx.cuda_ok(launch_deblock(fdev, nf, w, h, s), "deblocking")) return false;
   for (int f = 0; f < nf; f++)
     if (frames[f].dbg_si_final &&
         !ctx.cuda_ok(cudaMemcpyAsync(frames[f].dbg_si_final, fd[f].si, (size_t)w * h, cudaMemcpyDeviceToDevice, s),

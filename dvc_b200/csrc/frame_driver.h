@@ -32,6 +32,8 @@ struct FrameSpec {
   const uint8_t *acc = nullptr;   // host [qbits*w*h/128]
   uint8_t *recon = nullptr;       // device [w*h]; intra blocks filled in by the caller
   uint8_t *deblock_flag = nullptr;  // device [w*h] out, or null
+  int deblock = 0, intra_qp = 0;    // deblocking filter after decoding, with IntraQP thresholds
+  const uint8_t *past_mode = nullptr;  // host [w*h/64] modes of a WZ past reference, null for a key frame
   // optional device copies of intermediate stages (stage-level parity checks)
   uint8_t *dbg_si_initial = nullptr;  // side information after createSideInfo + intra copy
   float *dbg_alpha = nullptr;         // noise parameters
@@ -48,6 +50,7 @@ struct Slot {
   int w = 0, h = 0;
   DevBuf si, dbf, residue, side_trans, recons_trans, alpha, lr, oct, smf, pdf;
   DevBuf mb_mv, fmv, blk_mv, blk_mv2, holes, mse, stats, in, out;
+  DevBuf db_img, db_mode, db_bs;  // deblocking: filtered copy, per-edge mode and strength
   bool ensure(int w, int h, size_t pdf_floats, size_t in_bytes, size_t out_bytes);
   void release();
 };

@@ -28,6 +28,13 @@ struct FrameDev {
   double *holes, *mse;        // [b16n*2], [b88n]
   float *band_mean, *band_var;  // [16]
   int pdf_stride;             // floats per WZ block row of pdf
+  // deblocking (deblock.cpp:346-386): on/off, IntraQP, 2^(IntraQP/6) from the
+  // host's pow, the past reference's modes when it is a WZ frame
+  int deblock, db_qp, past_is_wz;
+  double db_pow;
+  const uint8_t *past_mode;   // [w*h/64]
+  uint8_t *db_img, *db_mode;  // [w*h] filtered copy; [2*w*h/16] edge mode (vertical edges, then horizontal)
+  double *db_bs;              // [2*w*h/16] edge strength
   int active;                 // 0: the descriptor is a placeholder, every kernel skips it
 };
 

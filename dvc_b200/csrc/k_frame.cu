@@ -997,6 +997,201 @@ __global__ void update_ml_kernel(FrameDev *frames, int band) {
 
 // ------------------------------------------------------------- launchers
 
+// ------------------------------------------------------------ deblocking
+//
+// The reference's deblocking filter (DvcDec/src/deblock.cpp:346-386): every
+// vertical 4x4 block edge in raster order, then every horizontal one, each
+// filtered from a decision taken on the frame before filtering
+// (deblock_44_decision, :228-344) with the strength and thresholds of the
+// H.264 in-loop filter.  Decisions are independent, so one thread takes each
+// edge; the filter of an edge touches up to three pixels on each side and
+// only its own pixel lines, so one thread walks each pixel row (vertical
+// edges) and then each pixel column (horizontal edges) in the reference's
+// order.
+
+// alpha, beta and tc0 by QP (H.264 tables 8-16 and 8-17; deblock.cpp:16-37)
+__constant__ uint8_t c_db_alpha[52] = {0,  0,  0,  0,  0,  0,  0,  0,  0,   0,   0,   0,   0,   0,   0,   0,   4,   4,
+                                       5,  6,  7,  8,  9,  10, 12, 13, 15,  17,  20,  22,  25,  28,  32,  36,  40,  45,
+                                       50, 56, 63, 71, 80, 90, 101, 113, 127, 144, 162, 182, 203, 226, 255, 255};
+__constant__ uint8_t c_db_beta[52] = {0, 0, 0, 0, 0, 0, 0, 0, 0,  0,  0,  0,  0,  0,  0,  0,  2,  2,
+                                      2, 3, 3, 3, 3, 4, 4, 4, 6,  6,  7,  7,  8,  8,  9,  9,  10, 10,
+                                      11, 11, 12, 12, 13, 13, 14, 14, 15, 15, 16, 16, 17, 17, 18, 18};
+__constant__ uint8_t c_db_tc0[52][3] = {
+    {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},    {0, 0, 0},    {0, 0, 0},    {0, 0, 0},    {0, 0, 0},
+    {0, 0, 0},   {0, 0, 0},   {0, 0, 0},   {0, 0, 0},    {0, 0, 0},    {0, 0, 0},    {0, 0, 0},    {0, 0, 0},
+    {0, 0, 0},   {0, 0, 1},   {0, 0, 1},   {0, 0, 1},    {0, 0, 1},    {0, 1, 1},    {0, 1, 1},    {1, 1, 1},
+    {1, 1, 1},   {1, 1, 1},   {1, 1, 1},   {1, 1, 2},    {1, 1, 2},    {1, 1, 2},    {1, 1, 2},    {1, 2, 3},
+    {1, 2, 3},   {2, 2, 3},   {2, 2, 4},   {2, 3, 4},    {2, 3, 4},    {3, 3, 5},    {3, 4, 6},    {3, 4, 6},
+    {4, 5, 7},   {4, 5, 8},   {4, 6, 9},   {5, 7, 10},   {6, 8, 11},   {6, 8, 13},   {7, 10, 14},  {8, 11, 16},
+    {9, 12, 18}, {10, 13, 20}, {11, 15, 23}, {13, 17, 25}};
+// quantiser table (reconstruction.cpp:9-43): the WZ-edge weights are Qtable[i] / sum
+__constant__ int c_db_qtable[9][16] = {
+    {0},
+    {16, 8, 0, 0, 8, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+    {32, 8, 0, 0, 8, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0},
+    {32, 8, 4, 0, 8, 4, 0, 0, 4, 0, 0, 0, 0, 0, 0, 0},
+    {32, 16, 8, 4, 16, 8, 4, 0, 8, 4, 0, 0, 4, 0, 0, 0},
+    {32, 16, 8, 4, 16, 8, 4, 4, 8, 4, 4, 0, 4, 4, 0, 0},
+    {64, 16, 8, 8, 16, 8, 8, 4, 8, 8, 4, 4, 8, 4, 4, 0},
+    {64, 32, 16, 8, 32, 16, 8, 4, 16, 8, 4, 4, 8, 4, 4, 0},
+    {128, 64, 32, 16, 64, 32, 16, 8, 32, 16, 8, 4, 16, 8, 4, 0}};
+
+#define DB_NONE 0
+#define DB_WZ 1    // both sides WZ blocks: strength from the reconstruction flags and variances
+#define DB_ISWZ 2  // an intra or skip side: H.264-style strength 1..4
+#define DB_BSMAX 0.14
+
+// weighted count of the coefficients reconstruction changed, and the
+// "flat block" indicator, of the 4x4 block at (bx, by) (deblock.cpp:286-327)
+__device__ void db_block_stats(const FrameDev &F, int bx, int by, double &phi, double &chi) {
+  const int *qt = c_db_qtable[F.qindex];
+  int qsum = 0;
+  for (int i = 0; i < 16; i++) qsum += qt[i];
+  phi = 0.0;
+  int sum = 0, sq = 0;
+  for (int m = 0; m < 4; m++) {
+    const int idx = ((by << 2) + m) * F.w + (bx << 2);
+    for (int n = 0; n < 4; n++) {
+      if (F.dbf[idx + n]) phi += (double)qt[(m << 2) + n] / (double)qsum;
+      const int v = F.recon[idx + n];
+      sum += v;
+      sq += v * v;
+    }
+  }
+  const double var = (double)sq / 16.0 - ((double)sum / 16.0) * ((double)sum / 16.0);
+  chi = var < 50.0 ? 1.0 : 0.0;
+}
+
+// deblock_44_decision (deblock.cpp:228-344) for the edge between 4x4 blocks 1 and 2
+__device__ int db_decide(const FrameDev &F, int x1, int y1, int x2, int y2, double &bs) {
+  const int b8w = F.w >> 3;
+  const int p1 = (y1 >> 1) * b8w + (x1 >> 1), p2 = (y2 >> 1) * b8w + (x2 >> 1);
+  const int t1 = F.mode[p1], t2 = F.mode[p2];
+  if (t1 == DVC_INTRA_B && t2 == DVC_INTRA_B) {
+    bs = 3.0;
+    return DB_ISWZ;
+  }
+  if (t1 == DVC_INTRA_B || t2 == DVC_INTRA_B) {
+    bs = (t1 == DVC_WZ_B || t2 == DVC_WZ_B) ? 4.0 : 3.0;
+    return DB_ISWZ;
+  }
+  if (t1 == DVC_SKIP_B && t2 == DVC_SKIP_B) {
+    bs = 0.0;
+    return DB_NONE;
+  }
+  if (t1 == DVC_SKIP_B || t2 == DVC_SKIP_B) {
+    if (F.past_is_wz) {
+      const int ps = t1 == DVC_SKIP_B ? p1 : p2;
+      bs = F.past_mode[ps] == DVC_INTRA_B ? 2.0 : 1.0;
+    } else {
+      bs = 2.0;
+    }
+    return DB_ISWZ;
+  }
+  double phi1, chi1, phi2, chi2;
+  db_block_stats(F, x1, y1, phi1, chi1);
+  db_block_stats(F, x2, y2, phi2, chi2);
+  const double P = 0.9;
+  bs = DB_BSMAX * (P * ((phi1 + phi2) / 2.0) + (1.0 - P) * ((chi1 + chi2) / 2.0));
+  return bs > 0.0 ? DB_WZ : DB_NONE;
+}
+
+// vertical edges at i*W4 + j (j < W4-1), horizontal edges at n + i*W4 + j (i < H4-1)
+__global__ void deblock_decide_kernel(FrameDev *frames) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !F.deblock) return;
+  const int w4 = F.w >> 2, h4 = F.h >> 2, n = w4 * h4;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 2 * n) return;
+  const int dir = e >= n, k = dir ? e - n : e, i = k / w4, j = k - i * w4;
+  double bs = 0.0;
+  int mode = DB_NONE;
+  if (dir == 0 ? j < w4 - 1 : i < h4 - 1) mode = dir == 0 ? db_decide(F, j, i, j + 1, i, bs) : db_decide(F, j, i, j, i + 1, bs);
+  F.db_mode[e] = (uint8_t)mode;
+  F.db_bs[e] = bs;
+}
+
+__device__ __forceinline__ int db_clip3(int lo, int hi, int x) { return x < lo ? lo : x > hi ? hi : x; }
+
+// deblock_filter (deblock.cpp:40-206) on one pixel line across one edge: p[0..7*st]
+// holds L3 L2 L1 L0 | R0 R1 R2 R3
+__device__ void db_line(uint8_t *p, int st, int mode, double bs, const FrameDev &F) {
+  const int alpha = c_db_alpha[F.db_qp], beta = c_db_beta[F.db_qp];
+  const int L3 = p[0], L2 = p[st], L1 = p[2 * st], L0 = p[3 * st];
+  const int R0 = p[4 * st], R1 = p[5 * st], R2 = p[6 * st], R3 = p[7 * st];
+  if (!(abs(R0 - L0) < alpha && abs(R0 - R1) < beta && abs(L0 - L1) < beta)) return;
+  const double mu = DB_BSMAX * 0.5;
+  const bool strong = mode == DB_ISWZ ? (int)bs == 4 : bs > mu;
+  if (strong) {
+    const int RL0 = L0 + R0;
+    const int small_gap = abs(R0 - L0) < ((alpha >> 2) + 2);
+    const int aq = (abs(R0 - R2) < beta) & small_gap, ap = (abs(L0 - L2) < beta) & small_gap;
+    if (ap) {
+      p[3 * st] = (uint8_t)((R1 + ((L1 + RL0) << 1) + L2 + 4) >> 3);
+      p[2 * st] = (uint8_t)((L2 + L1 + RL0 + 2) >> 2);
+      p[st] = (uint8_t)((((L3 + L2) << 1) + L2 + L1 + RL0 + 4) >> 3);
+    } else {
+      p[3 * st] = (uint8_t)(((L1 << 1) + L0 + R1 + 2) >> 2);
+    }
+    if (aq) {
+      p[4 * st] = (uint8_t)((L1 + ((R1 + RL0) << 1) + R2 + 4) >> 3);
+      p[5 * st] = (uint8_t)((R2 + R0 + L0 + R1 + 2) >> 2);
+      p[6 * st] = (uint8_t)((((R3 + R2) << 1) + R2 + R1 + RL0 + 4) >> 3);
+    } else {
+      p[4 * st] = (uint8_t)(((R1 << 1) + R0 + L1 + 2) >> 2);
+    }
+    return;
+  }
+  if (mode == DB_WZ && !(bs > 0.0)) return;
+  const int RL0 = (L0 + R0 + 1) >> 1;
+  const int aq = abs(R0 - R2) < beta, ap = abs(L0 - L2) < beta;
+  const int C0 = mode == DB_ISWZ ? (int)c_db_tc0[F.db_qp][(int)bs - 1] : (int)(bs * (F.db_pow - 1));
+  const int tc0 = C0 + ap + aq;
+  const int dif = db_clip3(-tc0, tc0, (((R0 - L0) << 2) + (L1 - R1) + 4) >> 3);
+  if (ap) p[2 * st] = (uint8_t)(p[2 * st] + db_clip3(-C0, C0, (L2 + RL0 - (L1 << 1)) >> 1));
+  p[3 * st] = (uint8_t)db_clip3(0, 255, L0 + dif);
+  p[4 * st] = (uint8_t)db_clip3(0, 255, R0 - dif);
+  if (aq) p[5 * st] = (uint8_t)(p[5 * st] + db_clip3(-C0, C0, (R2 + RL0 - (R1 << 1)) >> 1));
+}
+
+// pass 0: copy the frame; pass 1: vertical edges along each pixel row; pass 2:
+// horizontal edges down each pixel column; pass 3: copy the result back
+__global__ void deblock_pass_kernel(FrameDev *frames, int pass) {
+  FrameDev &F = frames[blockIdx.y];
+  if (!F.active || !F.deblock) return;
+  const int w = F.w, h = F.h, w4 = w >> 2, h4 = h >> 2, n = w4 * h4;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pass == 0) {
+    if (t < w * h) F.db_img[t] = F.recon[t];
+  } else if (pass == 1) {
+    if (t >= h) return;
+    const int i = t >> 2;
+    for (int j = 0; j < w4 - 1; j++) {
+      const int e = i * w4 + j;
+      if (F.db_mode[e] != DB_NONE) db_line(F.db_img + (size_t)t * w + (j << 2), 1, F.db_mode[e], F.db_bs[e], F);
+    }
+  } else if (pass == 2) {
+    if (t >= w) return;
+    const int j = t >> 2;
+    for (int i = 0; i < h4 - 1; i++) {
+      const int e = n + i * w4 + j;
+      if (F.db_mode[e] != DB_NONE) db_line(F.db_img + (size_t)(i << 2) * w + t, w, F.db_mode[e], F.db_bs[e], F);
+    }
+  } else {
+    if (t < w * h) F.recon[t] = F.db_img[t];
+  }
+}
+
+cudaError_t launch_deblock(FrameDev *fr, int nf, int w, int h, cudaStream_t s) {
+  const int n = (w / 4) * (h / 4);
+  deblock_decide_kernel<<<dim3((2 * n + 127) / 128, nf), 128, 0, s>>>(fr);
+  deblock_pass_kernel<<<dim3((w * h + 127) / 128, nf), 128, 0, s>>>(fr, 0);
+  deblock_pass_kernel<<<dim3((h + 127) / 128, nf), 128, 0, s>>>(fr, 1);
+  deblock_pass_kernel<<<dim3((w + 127) / 128, nf), 128, 0, s>>>(fr, 2);
+  deblock_pass_kernel<<<dim3((w * h + 127) / 128, nf), 128, 0, s>>>(fr, 3);
+  return cudaGetLastError();
+}
+
 static inline dim3 g2(int n, int tpb, int frames) { return dim3((n + tpb - 1) / tpb, frames); }
 
 cudaError_t launch_side_info(FrameDev *fr, int nf, int w, int h, cudaStream_t s) {

@@ -42,6 +42,8 @@ using Clock = std::chrono::steady_clock;
 struct Request {
   long long ticket = 0;
   int w = 0, h = 0, q = 0, past_idx = 0, future_idx = 0, cur_idx = 0, skip_mode = 0, intra_mode = 0;
+  int deblock = 0, intra_qp = 0;
+  std::vector<uint8_t> past_mode;  // empty: the past reference is a key frame
   int ac_range[16] = {0};
   std::vector<uint8_t> past, future, mode, crc, acc, recon;
   bool has_mode = false;
@@ -148,6 +150,9 @@ extern "C" int dvc_server_submit(dvc_server *S, const dvc_wz_frame *f, long long
   r->cur_idx = f->cur_idx;
   r->skip_mode = f->skip_mode;
   r->intra_mode = f->intra_mode;
+  r->deblock = f->deblock;
+  r->intra_qp = f->intra_qp;
+  if (f->past_mode) r->past_mode.assign(f->past_mode, f->past_mode + fs / 64);
   memcpy(r->ac_range, f->ac_range, sizeof r->ac_range);
   r->past.assign(f->past, f->past + fs);
   r->future.assign(f->future, f->future + fs);
@@ -256,6 +261,9 @@ static bool start_cohort(dvc_server *S, int i) {
     sp.mode = r.has_mode ? r.mode.data() : nullptr;
     sp.skip_mode = r.skip_mode;
     sp.intra_mode = r.intra_mode;
+    sp.deblock = r.deblock;
+    sp.intra_qp = r.intra_qp;
+    sp.past_mode = r.past_mode.empty() ? nullptr : r.past_mode.data();
     memcpy(sp.ac_range, r.ac_range, sizeof sp.ac_range);
     sp.crc = r.crc.data();
     sp.acc = r.acc.data();

@@ -21,10 +21,12 @@ def psnr(a, b):
 
 
 def frame_item(stream, fr, recon):
+    past_wz = stream.frames.get(fr.past)
     return dict(width=stream.width, height=stream.height, qindex=stream.qindex, past_idx=fr.past,
                 future_idx=fr.future, cur_idx=fr.idx, past=recon[fr.past], future=recon[fr.future],
                 mode=fr.mode, skip_mode=fr.skip_mode, intra_mode=fr.intra_mode, ac_range=fr.ac_range,
-                crc=fr.crc, acc=fr.acc_synd, recon=recon[fr.idx])
+                crc=fr.crc, acc=fr.acc_synd, recon=recon[fr.idx], deblock=stream.deblock,
+                intra_qp=stream.intra_qp, past_mode=None if past_wz is None else past_wz.mode)
 
 
 def decode_levels(stream, start=0, end=None):

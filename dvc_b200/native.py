@@ -73,7 +73,8 @@ class WZFrame(C.Structure):
                 ("skip_mode", C.c_int), ("intra_mode", C.c_int), ("ac_range", C.c_void_p),
                 ("crc", C.c_void_p), ("acc_synd", C.c_void_p), ("recon", C.c_void_p),
                 ("wz_bits", C.c_int), ("plane_results", C.c_void_p), ("plane_entropy", C.c_void_p),
-                ("deblock_flag", C.c_void_p)]
+                ("deblock_flag", C.c_void_p), ("deblock", C.c_int), ("intra_qp", C.c_int),
+                ("past_mode", C.c_void_p)]
 
 
 FRAME_API = {
@@ -204,10 +205,12 @@ class Context:
             crc = np.ascontiguousarray(it["crc"], np.uint8)
             acc = np.ascontiguousarray(it["acc"], np.uint8)
             rec = recs[i]
-            keep += [past, fut, mode, acr, crc, acc, rec]
+            pmode = None if it.get("past_mode") is None else np.ascontiguousarray(it["past_mode"], np.uint8)
+            keep += [past, fut, mode, acr, crc, acc, rec, pmode]
             arr[i] = WZFrame(w, h, it["qindex"], it["past_idx"], it["future_idx"], it["cur_idx"], _ptr(past),
                              _ptr(fut), _ptr(mode), it.get("skip_mode", 0), it.get("intra_mode", 0), _ptr(acr),
-                             _ptr(crc), _ptr(acc), _ptr(rec), 0, None, None, None)
+                             _ptr(crc), _ptr(acc), _ptr(rec), 0, None, None, None,
+                             it.get("deblock", 0), it.get("intra_qp", 0), _ptr(pmode))
             outs.append(len(crc))
         return arr, keep, outs
 
@@ -252,10 +255,12 @@ class Context:
             planes = np.zeros((qb, 4), np.int32)
             ent = np.zeros(qb, np.float32)
             dbf = np.zeros((h, w), np.uint8)
-            keep += [past, fut, mode, acr, crc, acc]
+            pmode = None if it.get("past_mode") is None else np.ascontiguousarray(it["past_mode"], np.uint8)
+            keep += [past, fut, mode, acr, crc, acc, pmode]
             arr[i] = WZFrame(w, h, it["qindex"], it["past_idx"], it["future_idx"], it["cur_idx"], _ptr(past),
                              _ptr(fut), _ptr(mode), it.get("skip_mode", 0), it.get("intra_mode", 0), _ptr(acr),
-                             _ptr(crc), _ptr(acc), _ptr(rec), 0, _ptr(planes), _ptr(ent), _ptr(dbf))
+                             _ptr(crc), _ptr(acc), _ptr(rec), 0, _ptr(planes), _ptr(ent), _ptr(dbf),
+                             it.get("deblock", 0), it.get("intra_qp", 0), _ptr(pmode))
             outs.append(dict(recon=rec, planes=planes, entropy=ent, deblock_flag=dbf))
         if debug:
             w, h = items[0]["width"], items[0]["height"]

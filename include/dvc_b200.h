@@ -119,6 +119,10 @@ typedef struct {
                                   iterations run (a work counter: it grows with the speculation width) */
   float *plane_entropy;        /* out [qbits] or NULL */
   uint8_t *deblock_flag;       /* out [w*h] or NULL: coefficients changed by reconstruction */
+  int deblock;                 /* 1: deblocking filter after decoding (the stream header's mode) */
+  int intra_qp;                /* IntraQP of the stream (deblocking thresholds) */
+  const uint8_t *past_mode;    /* [w*h/64] block modes of the past reference when it is a WZ
+                                  frame, NULL when it is a key frame (deblocking of skip blocks) */
 } dvc_wz_frame;
 
 /* Decode `count` WZ frames of one size as one batch on the device (frames

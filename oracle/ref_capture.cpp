@@ -14,7 +14,8 @@
 //   condBitProb         noiseModel.cpp:191         -> LR[] per bitplane
 //   ComputeCE           LdpcaDecoder.cpp:127       -> entropy per bitplane
 //   LdpcaDecoder        LdpcaDecoder.cpp:646       -> inputs/outputs per bitplane
-//   reconstruction      reconstruction.cpp:184     -> sideTrans after the call
+//   reconstruction      reconstruction.cpp:184     -> sideTrans and deblockFlag after the call
+//   deblock             deblock.cpp:346            -> frame, flags, modes, past index in; filtered frame out
 //   updateSI            sideInfoCreation.cpp:642   -> SI after the call
 #include <cstdio>
 #include <cstdlib>
@@ -132,6 +133,20 @@ void __wrap__Z14reconstructionPiS_iPfS_PhS1_(int *rt, int *st, int index, float 
   int32_t hdr[2] = {index, step[index]};
   rec("RECH", hdr, sizeof hdr);
   rec("STOU", st, FrameSize * 4);
+  rec("DBFL", dbf, FrameSize);
+}
+
+// ---- deblock(unsigned char *deblockimg, unsigned char *recon, unsigned char *deblockFlag, unsigned char *type_map, int begin)
+void __real__Z7deblockPhS_S_S_i(unsigned char *, unsigned char *, unsigned char *, unsigned char *, int);
+void __wrap__Z7deblockPhS_S_S_i(unsigned char *out, unsigned char *recon, unsigned char *flag, unsigned char *modes,
+                                int begin) {
+  rec("DBIN", recon, FrameSize);
+  rec("DBFG", flag, FrameSize);
+  rec("DBMD", modes, FrameSize / 64);
+  int32_t b = begin;
+  rec("DBBG", &b, 4);
+  __real__Z7deblockPhS_S_S_i(out, recon, flag, modes, begin);
+  rec("DBOU", out, FrameSize);
 }
 
 // ---- updateSI(SideInfo *si, unsigned char *recons, int current, int past, int future, SIR*)

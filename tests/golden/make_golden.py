@@ -18,7 +18,7 @@ decoder computed:
 The *_skip sequences are encoded with SkipBlock 1 on still-camera content, so
 their WZ frames carry JBIG-coded skip maps; the *_intra sequences with
 SkipBlock 1 and IntraMode 1, so they also carry intra maps and an intra
-bitstream (stored as ``intra``).
+bitstream (stored as ``intra``); the *_full sequences add DeblockingFilter 1.
 
 Usage (in the build container, after `make -C oracle ref` and
 `python oracle/ladder_dir.py oracle/_ref`):
@@ -38,7 +38,7 @@ from dvc_b200 import synth  # noqa: E402
 from oracle import refrun  # noqa: E402
 import ladders as lad  # noqa: E402
 
-# name: (kind, frames, gop, qindex, seed[, skip[, intra]])
+# name: (kind, frames, gop, qindex, seed[, skip[, intra[, deblock]]])
 SEQUENCES = {
     "qcif_g2_q4": ("qcif", 5, 2, 4, 11),
     "qcif_g4_q8": ("qcif", 5, 4, 8, 12),
@@ -49,10 +49,13 @@ SEQUENCES = {
     "qcif_g2_q4_intra": ("qcif", 5, 2, 4, 11, 1, 1),
     "cif_g4_q6_intra": ("cif", 5, 4, 6, 21, 1, 1),
     "qcif_g4_q8_allintra": ("qcif", 5, 4, 8, 12, 1, 1),
+    "qcif_g2_q4_full": ("qcif", 5, 2, 4, 11, 1, 1, 1),
+    "cif_g4_q6_full": ("cif", 5, 4, 6, 21, 1, 1, 1),
+    "qcif_still_g4_q4_full": ("qcif_still", 5, 4, 4, 41, 1, 1, 1),
 }
 
 
-def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0):
+def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0, deblock=0):
     w, h = synth.SHAPES[kind]
     size = "QCIF" if w == 176 else "CIF"
     ori, key = synth.make_sequence(kind, n_frames, seed)
@@ -62,7 +65,7 @@ def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0):
     synth.write_yuv420(oy, ori)
     synth.write_yuv420(ky, key)
     synth.write_frame_stat(st, n_frames)
-    wz, intra_bs, _ = refrun.encode(oy, ky, n_frames, size, gop, q, skip=skip, intra=intra)
+    wz, intra_bs, _ = refrun.encode(oy, ky, n_frames, size, gop, q, skip=skip, intra=intra, deblock=deblock)
     cap = os.path.join(d, "cap.bin")
     r = refrun.decode(oy, wz, intra_bs, ky, st, mode=0, capture=cap)
     dec_y = np.frombuffer(r["yuv"], np.uint8).reshape(-1, h, w)
