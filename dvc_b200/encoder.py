@@ -122,8 +122,24 @@ def accumulated_syndrome(L, src):
     return (np.bitwise_xor.accumulate((s & 1).astype(np.uint8))).astype(np.uint8)
 
 
-def encode_sequence(frames, gop, q, intra_qp=30, deblock=0):
-    """WZ bitstream (bytes) of a luma sequence with key frames every `gop` frames."""
+def skip_blocks(cur, past):
+    """8x8 blocks the reference encoder would skip: MSE against the past original
+    below 10 (DvcEnc/src/skipBlock.cpp:7-45, defines.h:10)."""
+    h, w = cur.shape
+    d = cur.astype(np.float64) - past.astype(np.float64)
+    mse = (d * d).reshape(h // 8, 8, w // 8, 8).sum(axis=(1, 3)) / 64.0
+    return mse < 10.0
+
+
+def encode_sequence(frames, gop, q, intra_qp=30, deblock=0, skip=0):
+    """WZ bitstream (bytes) of a luma sequence with key frames every `gop` frames.
+
+    skip=1 runs the encoder's skip test; a frame with no qualifying block keeps
+    skip mode off, as the reference does (its minimum-count rule cancels skip
+    mode, skipBlock.cpp:47-66).  Coding a frame that has skip blocks needs a
+    JBIG encoder, which this encoder does not have: it raises.  IntraMode is
+    always 0 (the reference then also leaves the deblocking filter to the
+    decoder, DVC_Encoder.cpp:41-81, so deblock only sets the header byte)."""
     t, h, w = frames.shape
     if (w, h) == (176, 144):
         res = 0
@@ -136,6 +152,8 @@ def encode_sequence(frames, gop, q, intra_qp=30, deblock=0):
     for i in range(0, t, gop):
         e = min(i + gop, t - 1)
         for (m, b, fe) in bs.gop_order(i, e):
+            if skip and skip_blocks(frames[m], frames[b]).any():
+                raise NotImplementedError("frame %d has skip blocks; coding its JBIG skip map is not implemented" % m)
             acr, crc, acc = encode_wz_frame(frames[m], q)
             for idx in bands:
                 out += bytes([(int(acr[idx]) >> 8) & 0xFF, int(acr[idx]) & 0xFF])
