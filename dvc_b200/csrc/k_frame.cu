@@ -830,10 +830,13 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   __shared__ int cur[16];
   __shared__ double scp[NT / 32], scf[NT / 32];
   __shared__ int sip[NT / 32], sif[NT / 32];
-  for (int k = threadIdx.x; k < ww * wh; k += NT) {
-    const int y = k / ww, x = k - y * ww;
-    wp[y * WS + x] = F.past[(st + y) * w + sl + x];
-    wf[y * WS + x] = F.future[(st + y) * w + sl + x];
+  // window rows by warp, pixels by lane (no per-pixel division)
+  for (int y = threadIdx.x >> 5; y < wh; y += NT / 32) {
+    const uint8_t *pp = F.past + (size_t)(st + y) * w + sl, *pf = F.future + (size_t)(st + y) * w + sl;
+    for (int x = threadIdx.x & 31; x < ww; x += 32) {
+      wp[y * WS + x] = pp[x];
+      wf[y * WS + x] = pf[x];
+    }
   }
   if (threadIdx.x < 16) cur[threadIdx.x] = F.recon[(top + (threadIdx.x >> 2)) * w + left + (threadIdx.x & 3)];
   __syncthreads();
@@ -885,42 +888,48 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   }
   block_argmin<NT>(bp, ip, scp, sip);
   block_argmin<NT>(bf, jf, scf, sif);
-  if (threadIdx.x == 0) {
-    int pbx = sl + ip % cw, pby = st + ip / cw, fbx = sl + jf % cw, fby = st + jf / cw;
-    // subPelRefine in the half-pel planes, no vector weight (sideInfoCreation.cpp:598-640)
-    for (int which = 0; which < 2; which++) {
-      const uint8_t *ref = which == 0 ? F.past_ip : F.future_ip;
-      int &bx = which == 0 ? pbx : fbx;
-      int &by = which == 0 ? pby : fby;
-      const int ix = bx << 1, iy = by << 1;
-      double minc = 10000000.0;
-      int nbx = bx, nby = by;
-      for (int di = -1; di <= 1; di++) {
-        const int tt = iy + di;
-        if (tt < 0 || tt > h2 - 8) continue;
-        for (int dj = -1; dj <= 1; dj++) {
-          const int ll = ix + dj;
-          if (ll < 0 || ll > w2 - 8) continue;
-          int sad = 0;
-          for (int m = 0; m < 4; m++)
-            for (int n = 0; n < 4; n++) sad += abs(cur[4 * m + n] - (int)ref[(tt + 2 * m) * w2 + ll + 2 * n]);
-          const double c = (double)sad;
-          if (c < minc) {
-            minc = c;
-            nbx = ll;
-            nby = tt;
-          }
-        }
-      }
-      bx = nbx;
-      by = nby;
+  // subPelRefine in the half-pel planes, no vector weight
+  // (sideInfoCreation.cpp:598-640): one thread per (reference, offset) SAD,
+  // then the strict-< scan over the offsets in the reference's (di, dj) order
+  __shared__ int ssad[18];
+  __shared__ int sbest[2][2];
+  const int t = threadIdx.x;
+  if (t < 18) {
+    const int which = t >= 9, k = t - 9 * which;
+    const int id = which ? jf : ip;
+    const int tt = ((st + id / cw) << 1) + k / 3 - 1, ll = ((sl + id % cw) << 1) + k % 3 - 1;
+    int sad = -1;  // offset outside the half-pel plane: not a candidate
+    if (tt >= 0 && tt <= h2 - 8 && ll >= 0 && ll <= w2 - 8) {
+      const uint8_t *ref = which ? F.future_ip : F.past_ip;
+      sad = 0;
+      for (int m = 0; m < 4; m++)
+        for (int n = 0; n < 4; n++) sad += abs(cur[4 * m + n] - (int)ref[(tt + 2 * m) * w2 + ll + 2 * n]);
     }
-    for (int m = 0; m < 4; m++)
-      for (int n = 0; n < 4; n++) {
-        const double pv = (double)F.past_ip[(pby + 2 * m) * w2 + pbx + 2 * n];
-        const double fv = (double)F.future_ip[(fby + 2 * m) * w2 + fbx + 2 * n];
-        F.si[(top + m) * w + left + n] = (uint8_t)(int)(pv * F.ipc + fv * F.ifc);
+    ssad[t] = sad;
+  }
+  __syncthreads();
+  if (t < 2) {
+    const int id = t ? jf : ip;
+    const int by = st + id / cw, bx = sl + id % cw;
+    double minc = 10000000.0;
+    int nbx = bx, nby = by;
+    for (int k = 0; k < 9; k++) {
+      const int sad = ssad[9 * t + k];
+      if (sad >= 0 && (double)sad < minc) {
+        minc = (double)sad;
+        nbx = (bx << 1) + k % 3 - 1;
+        nby = (by << 1) + k / 3 - 1;
       }
+    }
+    sbest[t][0] = nbx;
+    sbest[t][1] = nby;
+  }
+  __syncthreads();
+  if (t < 16) {
+    const int m = t >> 2, n = t & 3;
+    const double pv = (double)F.past_ip[(sbest[0][1] + 2 * m) * w2 + sbest[0][0] + 2 * n];
+    const double fv = (double)F.future_ip[(sbest[1][1] + 2 * m) * w2 + sbest[1][0] + 2 * n];
+    F.si[(top + m) * w + left + n] = (uint8_t)(int)(pv * F.ipc + fv * F.ifc);
   }
 }
 
