@@ -1,5 +1,6 @@
 // Decoder context set-up.  See context.h.
 #include "context.h"
+#include "exact_libm.h"
 
 #include <stdio.h>
 #include <stdlib.h>
@@ -86,16 +87,31 @@ bool Context::init(const char *data, const char *tables, int dev) {
   xlm.tanh_ylo = xlm_host.hdr.tanh_ylo;
   xlm.tanh_y1 = xlm_host.hdr.tanh_y1;
   {
-    // phi = -logf(tanhf(y)) for every float y in [tanh_ylo, tanh_y1), from the C library
+    // phi = -logf(tanhf(y)) for every float y in [tanh_ylo, tanh_y1), from the
+    // C library, swept and stored packed (every packed entry checked against the sweep)
     const size_t count = (size_t)xlm.tanh_y1 - xlm.tanh_ylo;
-    std::vector<float> phi(count);
-    dvc_phi_build(phi.data(), xlm.tanh_ylo, xlm.tanh_y1, 0);
-    void *p = nullptr;
-    if (cudaMalloc(&p, count * sizeof(float)) != cudaSuccess) return fail("phi table allocation failed");
-    xlm_allocs.push_back(p);
-    if (cudaMemcpy(p, phi.data(), count * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    PhiPacked pk;
+    {
+      std::vector<float> phi(count);
+      dvc_phi_build(phi.data(), xlm.tanh_ylo, xlm.tanh_y1, 0);
+      char perr[256];
+      if (!dvc_phi_pack(phi.data(), xlm.tanh_ylo, xlm.tanh_y1, 0, pk, perr, sizeof perr)) return fail(perr);
+    }
+    if (pk.desc.size() / 4 > XL_PHI_MAX_BINADES) return fail("phi table has too many binades");
+    auto put = [&](const void *src, size_t bytes, const void **dst) {
+      void *p = nullptr;
+      if (cudaMalloc(&p, bytes) != cudaSuccess) return false;
+      xlm_allocs.push_back(p);
+      if (cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return false;
+      *dst = p;
+      return true;
+    };
+    if (!put(pk.desc.data(), pk.desc.size() * 4, (const void **)&xlm.phi_desc) ||
+        !put(pk.rec.data(), pk.rec.size() * 4, (const void **)&xlm.phi_rec) ||
+        !put(pk.val.data(), pk.val.size() * 4, (const void **)&xlm.phi_val))
       return fail("uploading the phi table failed");
-    xlm.phi_tab = (const float *)p;
+    xlm.phi_nbin = (int)(pk.desc.size() / 4);
+    phi_bytes = (pk.desc.size() + pk.rec.size() + pk.val.size()) * 4;
   }
 
   // LDPCA ladders (QCIF n=1584 and CIF n=6336)

@@ -28,6 +28,7 @@ struct Context {
   XlmHost xlm_host;
   XlmDev xlm{};
   std::vector<void *> xlm_allocs;
+  size_t phi_bytes = 0;  // device bytes of the packed phi table
   std::vector<LadderHost> ladders_host;
   std::vector<LadderGpu> ladders_gpu;
   cudaStream_t stream = nullptr;

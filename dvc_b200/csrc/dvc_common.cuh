@@ -78,15 +78,35 @@ __device__ __forceinline__ float xl_expf(const XlmDev &t, const XlSmall &s, floa
   return xl_hash_lookup(t.exp_tab, t.exp_mask, t.exp_shift, u, m);
 }
 
+// copy the phi descriptors into shared memory (every thread of the block
+// calls this; follow with __syncthreads); `buf` holds XL_PHI_MAX_BINADES entries
+__device__ __forceinline__ void xl_phi_stage(const XlmDev &t, uint4 *buf) {
+  for (int i = threadIdx.x; i < t.phi_nbin; i += blockDim.x) buf[i] = t.phi_desc[i];
+}
+
 // -logf(tanhf(y)), the reference's two library calls (LdpcaDecoder.cpp:513,519),
-// from the direct table over [tanh_ylo, tanh_y1); -0 where tanhf(y) is 1.
+// from the packed table over [tanh_ylo, tanh_y1); -0 where tanhf(y) is 1.
 // Every argument the decoder forms is (x + 1e-9f)/2 with x >= 0, so it is at
 // least 5e-10 > 2^-31 = tanh_ylo; a smaller one (never formed) clamps to the
-// first entry rather than reading outside the table.
-__device__ __forceinline__ float xl_phi(const XlmDev &t, float y) {
+// first entry rather than reading outside the table.  `desc` is the binade
+// descriptor array (staged in shared memory by xl_phi_stage); one 16-byte
+// record read and one 4-byte value read (a rank value, or the first value
+// for delta binades, so that the code has no branch and the reads of several
+// calls can be in flight together).  Both are cached in L1: messages that
+// stay put from one iteration to the next read the same records again.
+__device__ __forceinline__ float xl_phi(const XlmDev &t, const uint4 *desc, float y) {
   const uint32_t u = __float_as_uint(y);
-  if (u >= t.tanh_y1) return -0.0f;  // also NaN/negative patterns, which the decoder never forms
-  return __ldg(t.phi_tab + (u > t.tanh_ylo ? u - t.tanh_ylo : 0u));
+  const bool one = u >= t.tanh_y1;  // tanhf(y) == 1 (also NaN/negative patterns, never formed)
+  const uint32_t i = (!one && u > t.tanh_ylo) ? u - t.tanh_ylo : 0u;
+  const uint4 d = desc[i >> XL_PHI_BINADE_BITS];
+  const uint32_t j = i & ((1u << XL_PHI_BINADE_BITS) - 1u);
+  const uint32_t g = xl_phi_group(j, d.z);
+  const uint4 r = __ldg(t.phi_rec + d.x + g);
+  const uint32_t f = xl_phi_field(j - g * (d.y & 0xffu), d.y, r.y, r.z, r.w);
+  const bool rank = (d.y & XL_PHI_RANK) != 0u;
+  const float rv = __ldg(t.phi_val + (rank ? r.x + f : 0u));
+  const float v = rank ? rv : __uint_as_float(r.x - f);
+  return one ? -0.0f : v;
 }
 
 }  // namespace dvc

@@ -34,8 +34,9 @@
 // The belief-propagation magnitude phi(y) = -logf(tanhf(y)) is not evaluated
 // at all: its argument is a float in [2^-31, y1) (y1 = the first float with
 // tanhf(y) == 1, above which phi is -0), so the library's value of the whole
-// expression is tabulated once per context for every one of those 2.9e8
-// floats (1.1 GB of device memory) and read with one load.
+// expression is swept once per context for every one of those 2.9e8 floats
+// and stored packed (xl_phi_field below, about 170 MB instead of 1.1 GB), so
+// that the part the decoder reads stays in the L2 cache.
 #pragma once
 #include <math.h>
 #include <stdint.h>
@@ -155,3 +156,59 @@ XL_HD uint32_t xl_tie_dist(double d) {
 #define XL_EXP_HI 0xc2d00000u  // -104.0f
 // tanh arguments y = (x + 1e-9)/2 with x >= 0, so y >= 5e-10
 #define XL_TANH_YLO 0x30000000u  // 2^-31, below the smallest y = 1e-9f/2 (0x3009705f)
+
+// ---- packed table of phi(y) = -logf(tanhf(y)) ----
+// Entry i is the library's phi of the float with bits XL_TANH_YLO + i.  The
+// entries are split into binades (2^23 consecutive patterns, one exponent of
+// y); each binade has a descriptor {first record, format, reciprocal} and is
+// cut into groups of G consecutive entries (4 <= G <= 32), one 16-byte record
+// per group: word 0 the group's base, words 1..3 (96 bits, word 1 lowest) G
+// fields of W = 96 / G bits, field k at bit k*W.  Field k is the offset of
+// entry k from the group's first entry (field 0 is 0):
+//  * delta format: base = bits of the group's first value, field k =
+//    bits(v_0) - bits(v_k) (phi falls as y grows), v_k = base - field k;
+//  * rank format (format bit 16): base = index in the value array of the
+//    group's first value, field k = how many times the value changes from
+//    entry 0 to entry k, v_k = values[base + field k]; used where the values
+//    jump by more than a field holds (large y, where tanhf takes few values)
+//    or where it is smaller.
+// One extract per read, the same for every format, so that lanes reading
+// different binades do not diverge.  The group of binade offset j is
+// j / G = umulhi(j, ceil(2^32 / G)) (exact for j < 2^23, G <= 32).  The
+// builder (libm_tables.cpp) picks the smallest feasible layout per binade and
+// checks every entry of the packed table against the swept one.
+#define XL_PHI_BINADE_BITS 23
+#define XL_PHI_RANK 0x10000u
+#define XL_PHI_MAX_BINADES 64
+
+XL_HD uint32_t xl_umulhi(uint32_t a, uint32_t b) {
+#if defined(__CUDA_ARCH__)
+  return __umulhi(a, b);
+#else
+  return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+}
+
+// group of binade offset j, recip = ceil(2^32 / G)
+XL_HD uint32_t xl_phi_group(uint32_t j, uint32_t recip) { return xl_umulhi(j, recip); }
+
+// field k of a record's words r1..r3; fmt = G | W << 8 | rank bit
+XL_HD uint32_t xl_phi_field(uint32_t k, uint32_t fmt, uint32_t r1, uint32_t r2, uint32_t r3) {
+  const uint32_t w = (fmt >> 8) & 0xffu;
+  const uint32_t p = k * w;
+  const uint32_t wi = p >> 5, sh = p & 31u;
+  const uint32_t lo = wi == 0 ? r1 : (wi == 1 ? r2 : r3);
+  const uint32_t hi = wi == 0 ? r2 : r3;
+#if defined(__CUDA_ARCH__)
+  return __funnelshift_r(lo, hi, sh) & ((1u << w) - 1u);
+#else
+  return (uint32_t)(((((uint64_t)hi) << 32) | lo) >> sh) & ((1u << w) - 1u);
+#endif
+}
+
+// value of entry k of a group from its record r0..r3 (host form of xl_phi)
+XL_HD float xl_phi_decode(uint32_t k, uint32_t fmt, uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3,
+                          const float *values) {
+  const uint32_t f = xl_phi_field(k, fmt, r1, r2, r3);
+  return (fmt & XL_PHI_RANK) ? values[r0 + f] : xl_bitsf(r0 - f);
+}

@@ -28,12 +28,12 @@
 // shared memory in the reference's summation order; columns (every column has
 // degree 3) reach their edges through the per-code position array.  The
 // parity check of an iteration's hard decision is folded into the next row
-// pass.  The magnitude phi(y) = -logf(tanhf(y)) is one read of the direct
-// table (dvc_common.cuh), and the reads of a pass are issued in batches so
-// that several are in flight per thread.  Shared memory is kept under 132 KB
-// so that the rest of the SM's 256 KB stays L1 cache: the per-code position
-// arrays and the table reads live there, and the L1 also bounds how many
-// table reads an SM can have in flight.
+// pass.  The magnitude phi(y) = -logf(tanhf(y)) is one record read of the
+// packed table (dvc_common.cuh; its hot part stays in L2), and the reads of a
+// pass are issued in batches so that several are in flight per thread.  Shared
+// memory is kept under 132 KB so that the rest of the SM's 256 KB stays L1
+// cache for the per-code position arrays and the table records that
+// successive iterations read again.
 //
 // Shared memory per codeword (n bits, e edges; CIF n=6336, e=19008: 124 KB):
 //   msg[e]  f32  edge messages by row-order position, in place:
@@ -147,7 +147,9 @@ __global__ void __launch_bounds__(NT, 1)
   uint8_t *dec = reinterpret_cast<uint8_t *>(rowt);  // decoded bits, once BP is over
   __shared__ uint32_t s_ured[NT / 32];
   __shared__ int s_start, s_accepted, s_stop;
+  __shared__ uint4 s_pdesc[XL_PHI_MAX_BINADES];
   const XlSmall xs = xl_small_global(xt);
+  xl_phi_stage(xt, s_pdesc);
 
   // accumulated syndrome bits (ByteToBit, LdpcaDecoder.cpp:81-107), entropy
   // terms H_k = (P(-log P + log(1-P)) - log(1-P)) / LOG2 with P = LR/(1+LR)
@@ -217,7 +219,8 @@ __global__ void __launch_bounds__(NT, 1)
     {
       float ph[MAXC];
 #pragma unroll
-      for (int c = 0; c < MAXC; c++) ph[c] = xl_phi(xt, (fabsf(llr[c]) + 1e-9f) / 2.0f);
+      for (int c = 0; c < MAXC; c++)
+        ph[c] = tid + c * NT < n ? xl_phi(xt, s_pdesc, (fabsf(llr[c]) + 1e-9f) / 2.0f) : 0.0f;
 #pragma unroll
       for (int c = 0; c < MAXC; c++) {
         const int k = tid + c * NT;
@@ -269,14 +272,11 @@ __global__ void __launch_bounds__(NT, 1)
         int rr[UNR];
 #pragma unroll
         for (int q = 0; q < UNR; q++) {
-          const int p = p0 + q * NT;
-          float y = 1.0f;
-          rr[q] = 0;
-          if (p < E) {
-            rr[q] = __ldg(rid + p);
-            y = (rowt[rr[q]] - msg[p] + 1e-9f) / 2.0f;
-          }
-          c[q] = xl_phi(xt, y);
+          // lanes past the last edge repeat it (no branch, so that the UNR
+          // table reads are in flight together) and store nothing
+          const int p = min(p0 + q * NT, E - 1);
+          rr[q] = __ldg(rid + p);
+          c[q] = xl_phi(xt, s_pdesc, (rowt[rr[q]] - msg[p] + 1e-9f) / 2.0f);
         }
 #pragma unroll
         for (int q = 0; q < UNR; q++) {
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(NT, 1)
             for (int i = 0; i < 3; i++) {
               const float v = tmp - mv[i];
               sb[b][i] = (__float_as_uint(v) >> 31) | (d << 1);
-              ph[b][i] = xl_phi(xt, (fabsf(v) + 1e-9f) / 2.0f);
+              ph[b][i] = xl_phi(xt, s_pdesc, (fabsf(v) + 1e-9f) / 2.0f);
             }
           }
         }
@@ -440,8 +440,14 @@ static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_j
   if (e != cudaSuccess) return e;
   const uint64_t bit = 1ull << (dev & 63);
   if (!(attr_set.load() & bit)) {
-    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)ldpca_smem_bytes(LDPCA_MAX_N, 3 * LDPCA_MAX_N));
+    const size_t most = ldpca_smem_bytes(LDPCA_MAX_N, 3 * LDPCA_MAX_N);
+    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most);
+    if (e != cudaSuccess) return e;
+    // the smallest shared-memory split that holds one block, so that the rest
+    // of the SM's 256 KB is L1 for the phi records, which BP iterations re-read
+    // (percent of the 228 KB maximum; the driver rounds up to a supported split)
+    const int pct = (int)(((most + 4096) * 100 + 228 * 1024 - 1) / (228 * 1024));
+    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
     if (e != cudaSuccess) return e;
     attr_set.fetch_or(bit);
   }

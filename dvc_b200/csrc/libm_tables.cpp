@@ -8,8 +8,8 @@
 //   expf   every float in [-104, -0]: hash of the differing pairs;
 //   tanhf  y1 = first float with tanhf(y) == 1 (checked to stay 1 above it);
 //   phi    -logf(tanhf(y)) for every y in [2^-31, y1), the belief-propagation
-//          magnitude, as one direct table (dvc_phi_build; not stored in the
-//          file, rebuilt in about a second when a context starts).
+//          magnitude (dvc_phi_build, packed by dvc_phi_pack; not stored in the
+//          file, rebuilt in about two seconds when a context starts).
 //
 // The file starts with the C library's version string; a loader that finds a
 // different version (or no file) rebuilds the tables.
@@ -222,4 +222,159 @@ void dvc_phi_build(float *out, uint32_t ylo, uint32_t y1, int threads) {
   parallel_ranges(ylo, (uint64_t)y1 - 1, threads, [&](int, uint64_t a, uint64_t b) {
     for (uint64_t u = a; u <= b; u++) out[u - ylo] = -logf(tanhf(xl_bitsf((uint32_t)u)));
   });
+}
+
+bool dvc_phi_pack(const float *phi, uint32_t ylo, uint32_t y1, int threads, PhiPacked &out, char *err, int errlen) {
+  if (threads <= 0) threads = hw_threads();
+  const uint32_t B = 1u << XL_PHI_BINADE_BITS;
+  if ((ylo & (B - 1)) != 0 || y1 <= ylo) {
+    snprintf(err, errlen, "phi table range [%08x, %08x) does not start a binade", ylo, y1);
+    return false;
+  }
+  const uint64_t n = (uint64_t)y1 - ylo;
+  const int nb = (int)((n + B - 1) / B);
+  auto bits = [&](uint64_t i) { return xl_fbits(phi[i]); };
+  std::atomic<int> next{0};
+  auto pool = [&](auto fn) {
+    next = 0;
+    std::vector<std::thread> ts;
+    for (int t = 0; t < threads; t++)
+      ts.emplace_back([&]() {
+        for (int b; (b = next.fetch_add(1)) < nb;) fn(b);
+      });
+    for (auto &th : ts) th.join();
+  };
+  // per binade: the smallest feasible layout.  G entries per record hold
+  // fields of W = 96 / G bits, so a group's span (delta: bits(v_0) - bits of
+  // its last value, which needs the binade to be non-increasing; rank: its
+  // number of changes) must stay below 2^W.  Rank with G = 4 always fits.
+  std::vector<uint32_t> fmt(nb);
+  std::vector<uint64_t> nrec(nb), nval(nb);
+  pool([&](int b) {
+    const uint64_t a = (uint64_t)b * B, e = std::min<uint64_t>(n, a + B), len = e - a;
+    std::vector<uint32_t> pre(len);  // changes in (a, a + t]
+    bool mono = true;
+    uint32_t c = 0;
+    pre[0] = 0;
+    for (uint64_t t = 1; t < len; t++) {
+      const uint32_t u0 = bits(a + t - 1), u1 = bits(a + t);
+      c += u1 != u0;
+      if (u1 > u0) mono = false;
+      pre[t] = c;
+    }
+    uint64_t best = ~0ull;
+    for (uint32_t G = 4; G <= 32; G++) {
+      const uint32_t W = 96 / G;
+      const uint64_t cap = (1ull << W) - 1, recs = (len + G - 1) / G;
+      uint64_t dmax = 0, rmax = 0;
+      for (uint64_t g0 = 0; g0 < len; g0 += G) {
+        const uint64_t g1 = std::min<uint64_t>(len, g0 + G) - 1;
+        dmax = std::max<uint64_t>(dmax, (uint64_t)bits(a + g0) - bits(a + g1));
+        rmax = std::max<uint64_t>(rmax, pre[g1] - pre[g0]);
+      }
+      if (mono && dmax <= cap && recs * 16 < best) {
+        best = recs * 16;
+        fmt[b] = G | (W << 8);
+        nrec[b] = recs;
+        nval[b] = 0;
+      }
+      if (rmax <= cap && recs * 16 + 4ull * (c + 1) < best) {
+        best = recs * 16 + 4ull * (c + 1);
+        fmt[b] = G | (W << 8) | XL_PHI_RANK;
+        nrec[b] = recs;
+        nval[b] = c + 1;
+      }
+    }
+  });
+  std::vector<uint64_t> rec0(nb + 1, 0), val0(nb + 1, 0);
+  for (int b = 0; b < nb; b++) {
+    rec0[b + 1] = rec0[b] + nrec[b];
+    val0[b + 1] = val0[b] + nval[b];
+  }
+  if (val0[nb] >= (1ull << 31) || rec0[nb] >= (1ull << 31)) {
+    snprintf(err, errlen, "phi table too large to pack");
+    return false;
+  }
+  out.desc.assign((size_t)nb * 4, 0);
+  for (int b = 0; b < nb; b++) {
+    const uint32_t G = fmt[b] & 0xffu;
+    out.desc[4 * b] = (uint32_t)rec0[b];
+    out.desc[4 * b + 1] = fmt[b];
+    out.desc[4 * b + 2] = (uint32_t)(((1ull << 32) + G - 1) / G);
+  }
+  out.rec.assign((size_t)rec0[nb] * 4, 0);
+  // at least one value: delta binades read (and discard) values[0]
+  out.val.assign(std::max<size_t>((size_t)val0[nb], 1), 0.0f);
+  pool([&](int b) {
+    const uint64_t a = (uint64_t)b * B, e = std::min<uint64_t>(n, a + B);
+    const uint32_t G = fmt[b] & 0xffu, W = (fmt[b] >> 8) & 0xffu;
+    const bool rank = (fmt[b] & XL_PHI_RANK) != 0;
+    uint32_t *rec = out.rec.data() + rec0[b] * 4;
+    uint64_t v = val0[b];
+    if (rank) out.val[v] = phi[a];
+    for (uint64_t g0 = a; g0 < e; g0 += G, rec += 4) {
+      if (rank && g0 > a && bits(g0) != bits(g0 - 1)) out.val[++v] = phi[g0];
+      rec[0] = rank ? (uint32_t)v : bits(g0);
+      uint32_t cnt = 0;
+      for (uint32_t k = 1; k < G && g0 + k < e; k++) {
+        const uint64_t i = g0 + k;
+        uint32_t f;
+        if (rank) {
+          if (bits(i) != bits(i - 1)) {
+            cnt++;
+            out.val[++v] = phi[i];
+          }
+          f = cnt;
+        } else {
+          f = bits(g0) - bits(i);
+        }
+        const uint32_t pos = k * W, wi = pos >> 5, sh = pos & 31u;
+        rec[1 + wi] |= f << sh;
+        if (sh + W > 32) rec[2 + wi] |= f >> (32 - sh);
+      }
+    }
+  });
+  // every entry of the packed table against the sweep, through the decode the device uses
+  std::atomic<uint64_t> bad{0}, first_bad{~0ull};
+  parallel_ranges(0, n - 1, threads, [&](int, uint64_t a, uint64_t e) {
+    for (uint64_t i = a; i <= e; i++) {
+      const uint32_t *d = out.desc.data() + 4 * (i >> XL_PHI_BINADE_BITS);
+      const uint32_t j = (uint32_t)(i & (B - 1)), g = xl_phi_group(j, d[2]);
+      const uint32_t *r = out.rec.data() + 4 * ((uint64_t)d[0] + g);
+      const float f = xl_phi_decode(j - g * (d[1] & 0xffu), d[1], r[0], r[1], r[2], r[3], out.val.data());
+      if (xl_fbits(f) != bits(i)) {
+        if (bad.fetch_add(1) == 0) first_bad = i;
+      }
+    }
+  });
+  if (bad.load()) {
+    snprintf(err, errlen, "packed phi table differs from the sweep at %llu entries (first %llu)",
+             (unsigned long long)bad.load(), (unsigned long long)first_bad.load());
+    return false;
+  }
+  return true;
+}
+
+extern "C" int dvc_phi_table_check(size_t *packed_bytes, char *msg, int msglen) {
+  // y1 = the first float with tanhf(y) == 1 (tanhf is non-decreasing)
+  uint32_t lo = XL_TANH_YLO, hi = 0x42000000u;  // tanhf(32) == 1
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (tanhf(xl_bitsf(mid)) == 1.0f) hi = mid;
+    else lo = mid + 1;
+  }
+  const uint32_t y1 = lo;
+  std::vector<float> phi((size_t)y1 - XL_TANH_YLO);
+  dvc_phi_build(phi.data(), XL_TANH_YLO, y1, 0);
+  PhiPacked pk;
+  char err[256];
+  if (!dvc_phi_pack(phi.data(), XL_TANH_YLO, y1, 0, pk, err, sizeof err)) {
+    if (msg && msglen > 0) snprintf(msg, (size_t)msglen, "%s", err);
+    return -4;  // DVC_E_DATA
+  }
+  if (packed_bytes) *packed_bytes = (pk.desc.size() + pk.rec.size() + pk.val.size()) * 4;
+  if (msg && msglen > 0)
+    snprintf(msg, (size_t)msglen, "%zu entries in %zu binades, %zu records, %zu rank values", phi.size(),
+             pk.desc.size() / 4, pk.rec.size() / 4, pk.val.size());
+  return 0;
 }

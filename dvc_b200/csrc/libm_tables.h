@@ -1,6 +1,7 @@
 // Correction tables for exact_libm.h: file layout, host loader, device view.
 #pragma once
 #include <stdint.h>
+#include <vector_types.h>
 
 #ifdef __cplusplus
 #include <vector>
@@ -30,7 +31,11 @@ typedef struct {
 typedef struct {
   const uint32_t *log_tab;
   const uint32_t *exp_tab;
-  const float *phi_tab;  // -logf(tanhf(y)) for y bits in [tanh_ylo, tanh_y1)
+  // -logf(tanhf(y)) for y bits in [tanh_ylo, tanh_y1), packed (exact_libm.h):
+  const uint4 *phi_desc;  // per binade: first record, format, ceil(2^32 / G), 0
+  const uint4 *phi_rec;   // 16-byte records
+  const float *phi_val;   // values of the rank-format binades (at least one)
+  int phi_nbin;           // binades (descriptors), at most XL_PHI_MAX_BINADES
   uint32_t log_mask, exp_mask;  // cap - 1
   int log_shift, exp_shift;     // 32 - log2(cap)
   uint32_t tanh_ylo, tanh_y1;
@@ -52,4 +57,14 @@ int dvc_libm_build(const char *path, int threads, char *err, int errlen);
 int dvc_libm_load(const char *path, XlmHost *out, char *err, int errlen);
 // out[i] = -logf(tanhf(y)) with the C library, y the float with bits ylo + i, i < y1 - ylo
 void dvc_phi_build(float *out, uint32_t ylo, uint32_t y1, int threads);
+
+// packed form of that table (exact_libm.h): desc holds 4 words per binade,
+// rec 4 words per record, val the rank values
+struct PhiPacked {
+  std::vector<uint32_t> desc, rec;
+  std::vector<float> val;
+};
+// Packs phi[0 .. y1 - ylo) (ylo must start a binade) and checks every entry
+// of the packed table against phi; returns false with a message on failure.
+bool dvc_phi_pack(const float *phi, uint32_t ylo, uint32_t y1, int threads, PhiPacked &out, char *err, int errlen);
 #endif

@@ -81,6 +81,15 @@ int dvc_jbig_decode_mode_map(const uint8_t *data, size_t len, int w, int h, uint
 int dvc_intra_decode_frame(const uint8_t *stream, size_t stream_bytes, size_t *bit_offset, int width, int height,
                            int intra_qp, const uint8_t *mode, uint8_t *recon);
 
+/* Self-check of the belief-propagation magnitude table, host code, no GPU:
+ * sweeps phi(y) = -logf(tanhf(y)) with this host's C library over every
+ * float argument the decoder can form, packs it the way dvc_create does for
+ * the device, and checks every packed entry against the sweep.  DVC_OK with
+ * *packed_bytes = the device bytes of the packed table; DVC_E_DATA with the
+ * reason in msg otherwise.  The reference has no counterpart: its decoder
+ * calls the two library functions per edge (LdpcaDecoder.cpp:513,519). */
+int dvc_phi_table_check(size_t *packed_bytes, char *msg, int msglen);
+
 /* LDPCA encoder on the device: for `count` source bitplanes of n bits
  * (bits[count*n], one 0/1 byte per bit) the accumulated syndromes acc[count*n/8]
  * (full-rate syndrome H*x, prefix-xored over the rows, packed MSB first as in
