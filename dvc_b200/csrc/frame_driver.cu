@@ -352,8 +352,10 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
     // speculation pays even on a full GPU (it shortens the slowest codeword of
-    // every lockstep bitplane step); at least 4 blocks per codeword, more when SMs are idle
-    int k = std::max(4, sms / std::max(1, std::max(nf, concurrent)));
+    // every lockstep bitplane step, for 7% more BP work at 8 blocks than at 1
+    // on 640 CIF frames, where 8 blocks decode 2x faster than 1 and 3% faster
+    // than 4 or 12); at least 8 blocks per codeword, more when SMs are idle
+    int k = std::max(8, sms / std::max(1, std::max(nf, concurrent)));
     if (const char *e = getenv("DVC_LDPCA_SPEC")) k = atoi(e);
     spec_k_ = std::max(1, std::min(32, k));
     if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_))) return ctx.fail("device allocation failed");
