@@ -848,7 +848,10 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   __syncthreads();
   // one thread per (reference, candidate column): the SAD of candidate row yo
   // is the sum over m of the 4-pixel SAD of window row yo + m against block
-  // row m, accumulated while walking the window rows once
+  // row m, accumulated while walking the window rows once.  The weight is at
+  // least 1, so cost = sad * weight >= sad (rounding is monotone): a candidate
+  // can only match or beat the item's best if sad <= floor(best), and only
+  // those are weighed; the rest could neither win nor tie.
   const int cw = sr - sl + 1;
   double bp = 1e300, bf = 1e300;
   int ip = 0x7fffffff, jf = 0x7fffffff;
@@ -861,6 +864,8 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     const int sh = (xo & 3) * 8;
     const double *wt = d_si_weight + (st - top + 32) * 65 + (sl + xo - left + 32);
     int part[4] = {0, 0, 0, 0};  // running SADs of candidate rows y-3 .. y (indexed by row & 3)
+    double best = 1e300;
+    int bi = 0x7fffffff, thr = 0x7fffffff;
     for (int y0 = 0; y0 < wh; y0 += 4) {
 #pragma unroll
       for (int r = 0; r < 4; r++) {
@@ -876,15 +881,20 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
           const int yo = y - 3;
           if (yo >= 0) {
             const int sad = part[(r - 3) & 3];
-            const double cst = (double)sad * __ldg(wt + yo * 65);
-            if (cst < 10000000.0) {
-              if (fut) better(bf, jf, cst, yo * cw + xo);
-              else better(bp, ip, cst, yo * cw + xo);
+            if (sad <= thr) {
+              const double cst = (double)sad * __ldg(wt + yo * 65);
+              if (cst < 10000000.0 && cst < best) {  // rows of an item come in increasing index order
+                best = cst;
+                bi = yo * cw + xo;
+                thr = (int)best;
+              }
             }
           }
         }
       }
     }
+    if (fut) better(bf, jf, best, bi);
+    else better(bp, ip, best, bi);
   }
   block_argmin<NT>(bp, ip, scp, sip);
   block_argmin<NT>(bf, jf, scf, sif);
