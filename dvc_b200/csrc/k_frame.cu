@@ -637,9 +637,10 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
   const int range = F.crange[index];
   const int blk = F.sir[s_idx];
   const int top = (blk / b4w) << 2, left = (blk % b4w) << 2;
+  constexpr int ML_N4 = (ML_N + 3) & ~3;
   __shared__ float etab[NOISE_TAB];
-  __shared__ float prob[ML_N];
-  __shared__ int sc[ML_N];
+  __shared__ __align__(16) float prob[ML_N4];
+  __shared__ __align__(16) int sc[ML_N4];
   __shared__ int s_n, s_dmax;
   const XlSmall xs = xl_small_global(xt);
   float *out = F.pdf + (size_t)s_idx * F.pdf_stride;
@@ -663,6 +664,12 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
     prob[q] = F.smf[(size_t)s_idx * ML_N + q];
     mx = max(mx, abs(v));
   }
+  // pad to a multiple of 4 with zero-probability terms: they add +0 to a
+  // non-negative sum, which leaves it unchanged
+  for (int q = ncand + threadIdx.x; q < ((ncand + 3) & ~3); q += NT) {
+    sc[q] = 0;
+    prob[q] = 0.0f;
+  }
   for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if ((threadIdx.x & 31) == 0) atomicMax(&s_dmax, mx);
   if (threadIdx.x == 0) s_n = ncand;
@@ -674,6 +681,26 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
   for (int d = threadIdx.x; d < tab; d += NT) etab[d] = xl_expf(xt, xs, -a * (float)d);
   __syncthreads();
   const int rmax = 2 * range + 1;
+  if (dmax < NOISE_TAB) {
+    // every distance is in the table: candidates four at a time, in order
+    const int nm4 = (nm + 3) >> 2;
+    const int4 *sc4 = reinterpret_cast<const int4 *>(sc);
+    const float4 *pr4 = reinterpret_cast<const float4 *>(prob);
+    for (int k = threadIdx.x; k < rmax; k += NT) {
+      const int pc = k - range;
+      float sum = 0.0f;
+      for (int m4 = 0; m4 < nm4; m4++) {
+        const int4 v = sc4[m4];
+        const float4 p = pr4[m4];
+        sum += p.x * etab[abs(pc - v.x)];
+        sum += p.y * etab[abs(pc - v.y)];
+        sum += p.z * etab[abs(pc - v.z)];
+        sum += p.w * etab[abs(pc - v.w)];
+      }
+      out[k] = sum;
+    }
+    return;
+  }
   for (int k = threadIdx.x; k < rmax; k += NT) {
     const int pc = k - range;
     float sum = 0.0f;
@@ -830,12 +857,17 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   __shared__ int cur[16];
   __shared__ double scp[NT / 32], scf[NT / 32];
   __shared__ int sip[NT / 32], sif[NT / 32];
-  // window rows by warp, pixels by lane (no per-pixel division)
+  // window rows by warp, aligned 4-byte words by lane: the window starts at
+  // byte `wo` of each shared row (w is a multiple of 4, so the words of
+  // [sl & ~3, sl + ww) stay inside the frame row; ww + 3 <= WS)
+  const int wo = sl & 3, nwd = (wo + ww + 3) >> 2;
   for (int y = threadIdx.x >> 5; y < wh; y += NT / 32) {
-    const uint8_t *pp = F.past + (size_t)(st + y) * w + sl, *pf = F.future + (size_t)(st + y) * w + sl;
-    for (int x = threadIdx.x & 31; x < ww; x += 32) {
-      wp[y * WS + x] = pp[x];
-      wf[y * WS + x] = pf[x];
+    const uint32_t *pp = reinterpret_cast<const uint32_t *>(F.past + (size_t)(st + y) * w + (sl - wo));
+    const uint32_t *pf = reinterpret_cast<const uint32_t *>(F.future + (size_t)(st + y) * w + (sl - wo));
+    uint32_t *dp = reinterpret_cast<uint32_t *>(wp + y * WS), *df = reinterpret_cast<uint32_t *>(wf + y * WS);
+    for (int x = threadIdx.x & 31; x < nwd; x += 32) {
+      dp[x] = __ldg(pp + x);
+      df[x] = __ldg(pf + x);
     }
   }
   if (threadIdx.x < 16) cur[threadIdx.x] = F.recon[(top + (threadIdx.x >> 2)) * w + left + (threadIdx.x & 3)];
@@ -860,8 +892,8 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     const bool fut = pc >= cw;
     const int xo = fut ? pc - cw : pc;
     const uint8_t *wb = fut ? wf : wp;
-    const uint32_t *row = reinterpret_cast<const uint32_t *>(wb) + (xo >> 2);
-    const int sh = (xo & 3) * 8;
+    const uint32_t *row = reinterpret_cast<const uint32_t *>(wb) + ((xo + wo) >> 2);
+    const int sh = ((xo + wo) & 3) * 8;
     const double *wt = d_si_weight + (st - top + 32) * 65 + (sl + xo - left + 32);
     int part[4] = {0, 0, 0, 0};  // running SADs of candidate rows y-3 .. y (indexed by row & 3)
     double best = 1e300;
