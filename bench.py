@@ -387,9 +387,12 @@ def main():
                                          "reads)" % alg_bytes_unit,
                          "units_per_launch": units_per_launch,
                          "aggregate_achieved": aggregate, "aggregate_frac": aggregate / peak,
-                         "note": "4-byte random gathers from a 1.1 GB table; each costs a 64-byte DRAM access, "
-                                 "and launches of 16 streams overlap, so the per-launch figure understates the "
-                                 "device-wide rate (aggregate_achieved: all launches of a step over the step time)"},
+                         "note": "4-byte phi values gathered at random from a packed 170 MB table whose hot part "
+                                 "stays in L2 (92% L2 hits, ~70 KB of DRAM traffic per block-iteration in ncu); the "
+                                 "kernel is bound by the latency of those L2 gathers and by L1TEX throughput, not by "
+                                 "DRAM bandwidth.  Launches of 16 streams overlap, so the per-launch figure "
+                                 "understates the device-wide rate (aggregate_achieved: all launches of a step over "
+                                 "the step time)"},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": int(prof["kernel_launches"]) * args.steps,
