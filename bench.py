@@ -3,24 +3,27 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload (one step): every WZ frame of 16 synthetic CIF 352x288 sequences, 65
-frames each: GOP 2 and GOP 4, each at QIndex 1..8 (SkipBlock 0, IntraMode 0,
-DeblockingFilter 1: the bench's encoder makes no skip or intra decisions;
-the decoder handles both, see tests), the seeded generator of dvc_b200.synth "cif" (six
+frames each: GOP 2 and GOP 4, each at QIndex 1..8 (SkipBlock 1, IntraMode 1,
+DeblockingFilter 1, IntraQP 30; skip and intra decisions by dvc_b200.encoder:
+the reference's skip test, which the moving content never passes, and a
+rate-based intra choice that picks none of the 8x8 blocks at Q1-2, about a
+tenth at Q4 and nearly all at Q8), the seeded generator of dvc_b200.synth "cif" (six
 sinusoids with periods 8-80 px, global motion, four moving 48x48 objects, key
 frames = original + N(0,2)) -> 8*32 + 8*48 = 640 WZ frames per step.  GOP-4
 frames 1 and 3 of each GOP take the decoded frame 2 as a reference, so a step
 has two levels of dependent frames.
 
 Our arm prints one JSON line with:
-  value   WZ frames/s of the batched device-resident path (dvc_session: inputs
-          already in HBM, cohorts of frames on concurrent streams, the GOP-4
-          levels chained on the device; device time from CUDA events; L2
-          flushed between steps);
+  value   WZ frames/s of the batched device-resident path (dvc_session: inputs,
+          intra pixels included, already in HBM, cohorts of frames on
+          concurrent streams, the GOP-4 levels chained on the device; device
+          time from CUDA events; L2 flushed between steps);
   e2e     the same through the public serving API with host buffers
-          (dvc_server: the frames of each level submitted at once, reference
-          frames, syndromes and CRCs copied in and decoded frames copied out
-          inside the timed region; the second level's references are the first
-          level's results);
+          (dvc_server: the host decode of the intra bitstreams, then the
+          frames of each level submitted at once, reference frames, starting
+          content, syndromes and CRCs copied in and decoded frames copied out,
+          all inside the timed region; the second level's references are the
+          first level's results);
   served  Poisson arrivals at fractions of the measured capacity through
           dvc_server (requests drawn from the first-level frames): throughput
           and per-frame latency p50/p99 (submit to completion);
@@ -52,25 +55,48 @@ GOPS = (2, 4)
 QS = tuple(range(1, 9))
 
 
+INTRA_QP = 30
+
+
 def workload():
-    """Original and key frames, and the parsed WZ stream of every (GOP, Q)."""
+    """Original and key frames, the parsed WZ stream and the intra bitstream of
+    every (GOP, Q)."""
     from dvc_b200 import bitstream as bs, encoder, synth
     ori, key = synth.make_sequence(KIND, N_FRAMES, SEED)
-    streams = {(g, q): bs.parse_wz(encoder.encode_sequence(ori, g, q, deblock=1)) for g in GOPS for q in QS}
-    return ori, key, streams
+    streams, intra_bs = {}, {}
+    for g in GOPS:
+        cache = {}  # the encoder's side-information estimate does not depend on Q
+        for q in QS:
+            wz, ib = encoder.encode_sequence_intra(ori, g, q, INTRA_QP, 1, 1, 1, si_cache=cache)
+            streams[(g, q)], intra_bs[(g, q)] = bs.parse_wz(wz), ib
+    return ori, key, streams, intra_bs
 
 
-def items(streams, key):
+def intra_starts(streams, intra_bs, key):
+    """Per (GOP, Q): the frames' starting content, key frames with the intra
+    blocks of each WZ frame decoded on the host (dvc_intra_decode_frame)."""
+    from dvc_b200 import intra
+    out = {}
+    for gq, st in streams.items():
+        start = np.array(key, np.uint8, copy=True)
+        for m, (px, _) in intra.decode_all(st, intra_bs[gq], key).items():
+            start[m] = px
+        out[gq] = start
+    return out
+
+
+def items(streams, key, starts):
     """Every WZ frame of every stream in decode order, as session items: a
     reference that is itself a WZ frame is named by the index of its item
-    (past_from / future_from); the level of each item is returned beside it."""
+    (past_from / future_from); the level of each item and its (GOP, Q, frame)
+    are returned beside it."""
     from dvc_b200 import decoder
-    out, level = [], []
+    out, level, src = [], [], []
     for (g, q), st in sorted(streams.items()):
         where = {}
         for lv, lvl in enumerate(decoder.decode_levels(st)):
             for (m, b, e) in lvl:
-                it = decoder.frame_item(st, st.frames[m], key)
+                it = decoder.frame_item(st, st.frames[m], starts[(g, q)])
                 for name, ref in (("past", b), ("future", e)):
                     if ref in st.frames:
                         it[name + "_from"] = where[ref]
@@ -78,7 +104,8 @@ def items(streams, key):
                 where[m] = len(out)
                 out.append(it)
                 level.append(lv)
-    return out, level
+                src.append(((g, q), m))
+    return out, level, src
 
 
 class Clocks:
@@ -135,10 +162,11 @@ def ref_cpu_sample(ori, key, streams, q, cores, workdir):
     synth.write_yuv420(ky, key[:3])
     synth.write_frame_stat(sf, 3)
     from dvc_b200 import encoder
+    wzb, ib = encoder.encode_sequence_intra(ori[:3], 2, q, INTRA_QP, 1, 1, 1)
     wz = os.path.join(d, "s.wz")
-    open(wz, "wb").write(encoder.encode_sequence(ori[:3], 2, q, deblock=1))
+    open(wz, "wb").write(wzb)
     intra = os.path.join(d, "s.intra")
-    open(intra, "wb").close()
+    open(intra, "wb").write(ib)
     t0 = time.time()
     r = refrun.decode(oy, wz, intra, ky, sf, mode=1 if cores > 1 else 0, cores=cores)
     wall = time.time() - t0
@@ -156,7 +184,7 @@ def run_reference(args, rank):
     if not refrun.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
         return
-    ori, key, streams = workload()
+    ori, key, streams, _ = workload()
     cores = os.cpu_count() or 1
     tmp = tempfile.mkdtemp()
     for i in range(args.warmup):
@@ -168,8 +196,8 @@ def run_reference(args, rank):
     line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": "WZ frames/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
-            "config": {"workload": "CIF 352x288 GOP2, one WZ frame per step, QIndex cycling 1..8, "
-                                   "reference DvcDec ParallelMode 1 on every host core",
+            "config": {"workload": "CIF 352x288 GOP2, one WZ frame per step, QIndex cycling 1..8, SkipBlock 1, "
+                                   "IntraMode 1, DeblockingFilter 1, reference DvcDec ParallelMode 1 on every host core",
                        "frames_per_step": 1},
             "cpu_baseline": {"value": fps, "unit": "WZ frames/s", "cores": cores, "kind": "reference",
                              "sample": "1 CIF WZ frame per step (3-frame GOP-2 sequence), Q cycling 1..8"},
@@ -201,8 +229,8 @@ def main():
     torch.cuda.set_device(local)
     from dvc_b200 import native
 
-    ori, key, streams = workload()
-    its, lev = items(streams, key)
+    ori, key, streams, intra_bs = workload()
+    its, lev, src = items(streams, key, intra_starts(streams, intra_bs, key))
     ctx = native.Context(local)
     ses = ctx.session(its, max_batch=args.max_batch, streams=args.streams)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
@@ -291,8 +319,13 @@ def main():
     for _ in range(max(1, args.steps)):
         flush.zero_()
         torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        starts = intra_starts(streams, intra_bs, key)  # the host part of the decode: intra blocks
+        for i, (gq, m) in enumerate(src):
+            its[i]["recon"] = starts[gq][m]
+        t_intra = time.perf_counter() - t0
         dt, _, served = serve_all()
-        e2e_t.append(dt)
+        e2e_t.append(t_intra + dt)
     barrier()
     e2e_s = replicas.max_over_ranks(float(np.mean(e2e_t)))
     # the served results equal the session's (both bit-exact paths), second level included
@@ -367,8 +400,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32/f64 (reference arithmetic, bit-exact)", "data": "synthetic",
             "config": {"workload": "CIF 352x288, 65-frame sequences at GOP 2 and GOP 4, QIndex 1..8 -> %d WZ "
-                                   "frames per step in two dependent levels (SkipBlock 0, IntraMode 0, "
-                                   "DeblockingFilter 1)"
+                                   "frames per step in two dependent levels (SkipBlock 1, IntraMode 1, "
+                                   "DeblockingFilter 1, IntraQP 30)"
                                    % frames_per_step,
                        "frames_per_step": frames_per_step, "max_batch": args.max_batch, "streams": args.streams,
                        "l2": "flushed (256 MB write) before every timed step",

@@ -302,7 +302,191 @@ void inverse44(int *b) {
 
 int round_half_away(double x) { return x >= 0.0 ? (int)(x + 0.5) : -(int)(-x + 0.5); }  // defines.h:23
 
+// ---- encoder side: the exact inverse of read_coeffs
+
+struct BitWriter {
+  uint8_t *d;
+  size_t nbits, pos;
+  bool over = false;
+  void bit(int b) {
+    if (pos >= nbits) {
+      over = true;
+      return;
+    }
+    const uint8_t m = (uint8_t)(0x80u >> (pos & 7));
+    if (b) d[pos >> 3] |= m;
+    else d[pos >> 3] &= (uint8_t)~m;
+    pos++;
+  }
+  void put(uint32_t v, int n) {
+    for (int i = n - 1; i >= 0; i--) bit((int)((v >> i) & 1u));
+  }
+  bool vlc(const Table &t, int sym) {
+    for (const Code &c : t)
+      if (c.sym == sym) {
+        put(c.bits, c.len);
+        return true;
+      }
+    return false;
+  }
+};
+
+// coefficients coeff[16] (raster positions of the 4x4 block) as CAVLC; false
+// when a value is outside what the syntax can carry
+bool write_coeffs(BitWriter &bw, const Frame &F, int bx, int by, std::vector<int> &nnz, const int coeff[16]) {
+  const Tables &T = tables();
+  int nc = 0, cnt = 0;
+  if (bx > 0 && F.intra(bx - 1, by)) {
+    nc += nnz[by * F.b4w + bx - 1];
+    cnt++;
+  }
+  if (by > 0 && F.intra(bx, by - 1)) {
+    nc += nnz[(by - 1) * F.b4w + bx];
+    cnt++;
+  }
+  if (cnt == 2) nc = (nc + 1) >> 1;
+  int level[16], pos[16], total = 0;
+  for (int p = 0; p < 16; p++) {
+    const int v = coeff[kZigzag[p]];
+    if (v) {
+      level[total] = v;
+      pos[total] = p;
+      total++;
+    }
+  }
+  int t1 = 0;
+  for (int k = total - 1; k >= 0 && t1 < 3 && (level[k] == 1 || level[k] == -1); k--) t1++;
+  nnz[by * F.b4w + bx] = total;
+  if (nc >= 8) {
+    bw.put(total == 0 ? 3u : (uint32_t)(((total - 1) << 2) | t1), 6);
+  } else if (!bw.vlc(T.coeff[nc < 2 ? 0 : nc < 4 ? 1 : 2], total * 4 + t1)) {
+    return false;
+  }
+  if (total == 0) return true;
+  for (int k = total - 1; k >= total - t1; k--) bw.bit(level[k] < 0 ? 1 : 0);
+  int suffix_len = (total > 10 && t1 < 3) ? 1 : 0;
+  for (int k = total - 1 - t1; k >= 0; k--) {
+    const int v = level[k];
+    int code = v > 0 ? 2 * v - 2 : -2 * v - 1;
+    if (k == total - 1 - t1 && t1 < 3) code -= 2;
+    if (suffix_len == 0) {
+      if (code < 14) {
+        bw.put(1u, code + 1);
+      } else if (code < 30) {
+        bw.put(1u, 15);
+        bw.put((uint32_t)(code - 14), 4);
+      } else {
+        if (code - 30 >= 4096) return false;
+        bw.put(1u, 16);
+        bw.put((uint32_t)(code - 30), 12);
+      }
+    } else if (code < (15 << suffix_len)) {
+      bw.put(1u, (code >> suffix_len) + 1);
+      bw.put((uint32_t)(code & ((1 << suffix_len) - 1)), suffix_len);
+    } else {
+      if (code - (15 << suffix_len) >= 4096) return false;
+      bw.put(1u, 16);
+      bw.put((uint32_t)(code - (15 << suffix_len)), 12);
+    }
+    int sl = suffix_len == 0 ? 1 : suffix_len;
+    const int a = v < 0 ? -v : v;
+    if (a > (3 << (sl - 1)) && sl < 6) sl++;
+    if (k == total - 1 - t1 && a > 3) sl = 2;
+    suffix_len = sl;
+  }
+  if (total < 16) {
+    const int zeros = pos[total - 1] + 1 - total;
+    if (!bw.vlc(T.total_zeros[total - 1], zeros)) return false;
+    int left = zeros;
+    for (int i = total - 1; i > 0 && left > 0; i--) {
+      const int run = pos[i] - pos[i - 1] - 1;
+      if (!bw.vlc(T.run_before[std::min(left, 7) - 1], run)) return false;
+      left -= run;
+    }
+  }
+  return true;
+}
+
 }  // namespace
+
+namespace {
+
+// DC prediction from the reconstructed intra neighbours of block (bx, by)
+int dc_pred(const Frame &F, const uint8_t *recon, int bx, int by) {
+  const int top = by * 4, left = bx * 4, width = F.w;
+  const bool up = by > 0 && F.intra(bx, by - 1), lf = bx > 0 && F.intra(bx - 1, by);
+  int s = 0;
+  if (up)
+    for (int j = 0; j < 4; j++) s += recon[(top - 1) * width + left + j];
+  if (lf)
+    for (int i = 0; i < 4; i++) s += recon[(top + i) * width + left - 1];
+  return (up && lf) ? (s + 4) >> 3 : (up || lf) ? (s + 2) >> 2 : 128;
+}
+
+}  // namespace
+
+extern "C" int dvc_intra_encode_frame(const uint8_t *ori, int width, int height, int intra_qp, const uint8_t *mode,
+                                      uint8_t *stream, size_t stream_bytes, size_t *bit_offset, uint8_t *recon,
+                                      int *block_bits) {
+  if (!ori || !stream || !bit_offset || !mode || !recon ||
+      !((width == 176 && height == 144) || (width == 352 && height == 288)) || intra_qp < 0 || intra_qp > 51)
+    return DVC_E_ARG;
+  if (!tables().ok) return DVC_E_DATA;
+  Frame F{width, height, width / 4, height / 4, width / 8, mode};
+  BitWriter bw{stream, stream_bytes * 8, *bit_offset};
+  // the decoder's de-quantisation scale, computed the same way
+  const double qstep = pow(2.0, ((double)intra_qp - 4.0) / 6.0);
+  const double a2 = 0.25, b2 = 0.4, ab = 0.5 * sqrt(0.4);
+  const double pre[16] = {a2, ab, a2, ab, ab, b2, ab, b2, a2, ab, a2, ab, ab, b2, ab, b2};
+  // forward normalisation of the core transform: a^2, ab/2, b^2/4 (a = 1/2, b = sqrt(2/5))
+  const double ea = 0.25, eb = 0.1, eab = 0.25 * sqrt(0.4);
+  const double ef[16] = {ea, eab, ea, eab, eab, eb, eab, eb, ea, eab, ea, eab, eab, eb, eab, eb};
+  std::vector<int> nnz((size_t)F.b4w * F.b4h, 0);
+  for (int by = 0; by < F.b4h; by++)
+    for (int bx = 0; bx < F.b4w; bx++) {
+      if (!F.intra(bx, by)) continue;
+      const int top = by * 4, left = bx * 4;
+      const int pred = dc_pred(F, recon, bx, by);
+      int x[16], t[16], coeff[16], blk[16];
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) x[4 * i + j] = (int)ori[(top + i) * width + left + j] - pred;
+      // core transform rows then columns: Cf X Cf^T
+      for (int i = 0; i < 4; i++) {
+        const int *r = x + 4 * i;
+        t[4 * i] = r[0] + r[1] + r[2] + r[3];
+        t[4 * i + 1] = 2 * r[0] + r[1] - r[2] - 2 * r[3];
+        t[4 * i + 2] = r[0] - r[1] - r[2] + r[3];
+        t[4 * i + 3] = r[0] - 2 * r[1] + 2 * r[2] - r[3];
+      }
+      for (int j = 0; j < 4; j++) {
+        const int c0 = t[j], c1 = t[4 + j], c2 = t[8 + j], c3 = t[12 + j];
+        x[j] = c0 + c1 + c2 + c3;
+        x[4 + j] = 2 * c0 + c1 - c2 - 2 * c3;
+        x[8 + j] = c0 - c1 - c2 + c3;
+        x[12 + j] = c0 - 2 * c1 + 2 * c2 - c3;
+      }
+      // quantisation with a one-third rounding offset, as intra coders use
+      for (int i = 0; i < 16; i++) {
+        const double y = (double)x[i] * ef[i] / qstep;
+        const int q = (int)(fabs(y) + 1.0 / 3.0);
+        coeff[i] = y < 0 ? -q : q;
+      }
+      const size_t before = bw.pos;
+      if (!write_coeffs(bw, F, bx, by, nnz, coeff)) return DVC_E_ARG;
+      if (block_bits) block_bits[by * F.b4w + bx] = (int)(bw.pos - before);
+      // the decoder's reconstruction, so that later blocks predict from it
+      for (int i = 0; i < 16; i++) blk[i] = round_half_away((double)coeff[i] * qstep * (pre[i] * 64.0));
+      inverse44(blk);
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+          const int v = blk[4 * i + j] + pred;
+          recon[(top + i) * width + left + j] = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
+        }
+    }
+  if (bw.over) return DVC_E_ARG;
+  *bit_offset = bw.pos;
+  return DVC_OK;
+}
 
 extern "C" int dvc_intra_decode_frame(const uint8_t *stream, size_t stream_bytes, size_t *bit_offset, int width,
                                       int height, int intra_qp, const uint8_t *mode, uint8_t *recon) {

@@ -18,6 +18,9 @@
 //    other byte is a marker that ends the data, after which the decoder reads
 //    zero bytes; SDNORM (0xFF 0x02) or SDRST (0xFF 0x03) closes the stripe.
 //
+// The encoder (dvc_jbig_encode_mode_map) writes the same form: the coded
+// stripe of the map with the same template and options, closed by SDNORM.
+//
 // An adaptive-template move (ATMOVE marker) is refused: the reference encoder
 // does not emit one for maps of these sizes (none in thousands of maps coded
 // by it), and a stream that had one would decode wrongly here.
@@ -138,7 +141,120 @@ struct QmDecoder {
   }
 };
 
+// QM encoder (T.82 6.8): the interval register C holds, from bit 27 down, a
+// carry bit, the 8 bits of the next output byte, 3 spacer bits and the 16
+// bits aligned with A.  Output bytes are held back one at a time (`buffer`)
+// and runs of 0xFF are only counted (`stacked`), so that a carry out of C can
+// still propagate into them; every 0xFF written is followed by a 0x00 stuff
+// byte.
+struct QmEncoder {
+  std::vector<uint8_t> out;
+  uint32_t c = 0, a = 0x10000;
+  int ct = 11, stacked = 0, buffer = -1;
+  uint8_t st[1024] = {0}, mps[1024] = {0};
+
+  void put(int b) {
+    out.push_back((uint8_t)b);
+    if (b == 0xFF) out.push_back(0x00);
+  }
+  void byte_out() {
+    const uint32_t t = c >> 19;
+    if (t > 0xFF) {  // carry: the held byte grows by one, the stacked 0xFF become 0x00
+      if (buffer >= 0) put(buffer + 1);
+      for (; stacked > 0; stacked--) out.push_back(0x00);
+      buffer = (int)(t & 0xFF);
+    } else if (t == 0xFF) {
+      stacked++;
+    } else {
+      if (buffer >= 0) put(buffer);
+      for (; stacked > 0; stacked--) put(0xFF);
+      buffer = (int)t;
+    }
+    c &= 0x7FFFF;
+  }
+  void renorm() {
+    do {
+      a <<= 1;
+      c <<= 1;
+      if (--ct == 0) {
+        byte_out();
+        ct = 8;
+      }
+    } while (a < 0x8000);
+  }
+  // the upper sub-interval of size Qe belongs to the LPS unless A - Qe < Qe,
+  // in which case the two sub-intervals swap (conditional exchange)
+  void encode(int cx, int pix) {
+    const int s = st[cx];
+    const uint32_t q = kQe[s];
+    a -= q;
+    if (pix == mps[cx]) {
+      if (a >= 0x8000) return;
+      if (a < q) {
+        c += a;
+        a = q;
+      }
+      st[cx] = kNextMps[s];
+    } else {
+      if (a >= q) {
+        c += a;
+        a = q;
+      }
+      if (kSwitch[s]) mps[cx] = (uint8_t)(1 - mps[cx]);
+      st[cx] = kNextLps[s];
+    }
+    renorm();
+  }
+  // pick the value in [C, C + A) with the most trailing zero bits, write out
+  // what is left, and drop final bytes that are 0x00 (a decoder reads zeros
+  // past the end of the data)
+  void flush() {
+    const uint32_t t = (a - 1 + c) & 0xFFFF0000u;
+    c = t < c ? t + 0x8000 : t;
+    c <<= ct;
+    if (c & 0xF8000000u) {
+      if (buffer >= 0) put(buffer + 1);
+      if (c & 0x7FFF800u)
+        for (; stacked > 0; stacked--) out.push_back(0x00);
+    } else {
+      if (buffer >= 0) put(buffer);
+      for (; stacked > 0; stacked--) put(0xFF);
+    }
+    if (c & 0x7FFF800u) {
+      put((int)((c >> 19) & 0xFF));
+      if (c & 0x7F800u) put((int)((c >> 11) & 0xFF));
+    }
+  }
+};
+
 }  // namespace
+
+extern "C" int dvc_jbig_encode_mode_map(const uint8_t *map, int w, int h, uint8_t *out, size_t cap, size_t *len) {
+  if (!map || !out || !len || w <= 0 || h <= 0 || w > 4096 || h > 4096) return DVC_E_ARG;
+  QmEncoder q;
+  const int W = w + 4;
+  std::vector<uint8_t> r2(W, 0), r1(W, 0), r0(W, 0);
+  for (int y = 0; y < h; y++) {
+    std::fill(r0.begin(), r0.end(), 0);
+    for (int x = 0; x < w; x++) {
+      const int X = x + 2;
+      const int cx = (r2[X - 1] << 9) | (r2[X] << 8) | (r2[X + 1] << 7) | (r1[X - 2] << 6) | (r1[X - 1] << 5) |
+                     (r1[X] << 4) | (r1[X + 1] << 3) | (r1[X + 2] << 2) | (r0[X - 2] << 1) | r0[X - 1];
+      const int pix = map[(size_t)y * w + x] ? 1 : 0;
+      q.encode(cx, pix);
+      r0[X] = (uint8_t)pix;
+    }
+    r2.swap(r1);
+    r1.swap(r0);
+  }
+  q.flush();
+  q.out.push_back(0xFF);  // SDNORM closes the stripe
+  q.out.push_back(0x02);
+  *len = q.out.size();
+  if (q.out.size() > cap) return DVC_E_ARG;
+  memcpy(out, q.out.data(), q.out.size());
+  return DVC_OK;
+}
 
 extern "C" int dvc_jbig_decode_mode_map(const uint8_t *data, size_t len, int w, int h, uint8_t *map, size_t *used) {
   if (!data || !map || w <= 0 || h <= 0 || w > 4096 || h > 4096) return DVC_E_ARG;

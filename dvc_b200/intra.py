@@ -39,3 +39,24 @@ def decode_all(stream, intra_bytes, base_frames=None):
             raise ValueError("intra bitstream of frame %d could not be decoded (status %d)" % (m, rc))
         out[m] = (rec, off.value - before)
     return out
+
+
+def encode_frame(ori, mode88, intra_qp, buf, bit_offset, with_bits=False):
+    """Append the intra blocks of one frame (mode88 [H/8, W/8], 1 = intra) to the
+    bit string in `buf` (a writable uint8 array) at bit_offset.  Returns (new
+    bit offset, uint8 [H, W] with the intra blocks as the decoder reconstructs
+    them, other pixels 0) and, with_bits, the bits of each 4x4 block
+    [H/4, W/4]."""
+    ori = np.ascontiguousarray(ori, np.uint8)
+    h, w = ori.shape
+    mode = np.ascontiguousarray(np.asarray(mode88) != 0, np.uint8)
+    rec = np.zeros((h, w), np.uint8)
+    bits = np.zeros((h // 4, w // 4), np.int32)
+    off = C.c_size_t(bit_offset)
+    rc = native.lib().dvc_intra_encode_frame(ori.ctypes.data_as(C.c_void_p), w, h, intra_qp,
+                                            mode.ctypes.data_as(C.c_void_p), buf.ctypes.data_as(C.c_void_p),
+                                            len(buf), C.byref(off), rec.ctypes.data_as(C.c_void_p),
+                                            bits.ctypes.data_as(C.c_void_p))
+    if rc != native.DVC_OK:
+        raise ValueError("intra blocks could not be encoded (status %d)" % rc)
+    return (off.value, rec, bits) if with_bits else (off.value, rec)

@@ -3,7 +3,8 @@
 The reference codes each frame's 8x8 skip and intra maps with JBIG-KIT and
 stores the coded stripe without its header (DvcEnc/src/wzbitstream.cpp:28-44);
 ``decode_mode_map`` returns the map and the bytes the stripe occupies, as the
-reference's reader does (DvcDec/src/wzbitstream.cpp:38-66).
+reference's reader does (DvcDec/src/wzbitstream.cpp:38-66); ``encode_mode_map``
+writes the same bytes as the reference's writer.
 """
 import ctypes as C
 
@@ -22,3 +23,17 @@ def decode_mode_map(buf, w, h):
     if rc != native.DVC_OK:
         raise ValueError("JBIG mode map could not be decoded (status %d)" % rc)
     return out, used.value
+
+
+def encode_mode_map(m):
+    """Coded bytes (stripe data and the closing SDNORM marker) of a 0/1 map [h, w]."""
+    m = np.ascontiguousarray(np.asarray(m, np.uint8) != 0, np.uint8)
+    h, w = m.shape
+    cap = 2 * w * h + 64
+    out = np.zeros(cap, np.uint8)
+    n = C.c_size_t(0)
+    rc = native.lib().dvc_jbig_encode_mode_map(m.ctypes.data_as(C.c_void_p), w, h, out.ctypes.data_as(C.c_void_p),
+                                               cap, C.byref(n))
+    if rc != native.DVC_OK:
+        raise ValueError("JBIG mode map could not be encoded (status %d)" % rc)
+    return out[:n.value].tobytes()

@@ -95,7 +95,10 @@ FRAME_API = {
     "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
     "dvc_ldpca_encode": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p],
     "dvc_phi_table_check": [C.POINTER(C.c_size_t), C.c_char_p, C.c_int],
+    "dvc_jbig_encode_mode_map": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
     "dvc_jbig_decode_mode_map": [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)],
+    "dvc_intra_encode_frame": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_size_t,
+                               C.POINTER(C.c_size_t), C.c_void_p, C.c_void_p],
     "dvc_intra_decode_frame": [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_int, C.c_int, C.c_int, C.c_void_p,
                                C.c_void_p],
 }

@@ -69,6 +69,15 @@ int dvc_ldpca_decode(dvc_ctx *ctx, int n, int count, const float *lr, const uint
  * DVC_E_DATA for a truncated stream or a stream with an adaptive-template move. */
 int dvc_jbig_decode_mode_map(const uint8_t *data, size_t len, int w, int h, uint8_t *map, size_t *used);
 
+/* JBIG (T.82) encoder for a skip or intra mode map: map[h*w] (nonzero = the
+ * 8x8 block has the mode) coded as the reference encoder stores it after a set
+ * skipMode / intraMode byte, the coded stripe closed by SDNORM, into out[cap];
+ * *len = its length (also when cap is too small, which returns DVC_E_ARG).
+ * Replaces simple_JBIG_enc over JBIG-KIT (DvcEnc/src/sJBIG.cpp:54-71, called
+ * at wzbitstream.cpp:36-50) and gives the same bytes; the length is also what
+ * the reference's skip-count rule uses (skipBlock.cpp:47-66).  Host code. */
+int dvc_jbig_encode_mode_map(const uint8_t *map, int w, int h, uint8_t *out, size_t cap, size_t *len);
+
 /* Intra blocks of one WZ frame (IntraMode 1), decoded from the sequence's
  * intra bitstream: CAVLC coefficients, de-quantisation with IntraQP, 4x4
  * inverse transform, DC prediction from intra neighbours; the pixels of every
@@ -80,6 +89,21 @@ int dvc_jbig_decode_mode_map(const uint8_t *data, size_t len, int w, int h, uint
  * DVC_E_DATA on a malformed or exhausted bitstream. */
 int dvc_intra_decode_frame(const uint8_t *stream, size_t stream_bytes, size_t *bit_offset, int width, int height,
                            int intra_qp, const uint8_t *mode, uint8_t *recon);
+
+/* Intra blocks of one WZ frame into the intra bitstream: for every 4x4 block
+ * inside an intra 8x8 block (mode[w*h/64] == 1), in raster order, DC
+ * prediction from the reconstructed intra neighbours, the 4x4 core transform,
+ * quantisation with IntraQP and CAVLC, appended at *bit_offset of
+ * stream[stream_bytes] (advanced past the frame's blocks); recon[w*h] receives
+ * the pixels dvc_intra_decode_frame will reconstruct, and block_bits (if not
+ * NULL, one int per 4x4 block) the bits each intra block took.  The counterpart of the
+ * reference encoder's real_intra (DvcEnc/src/intra.cpp, vlc.cpp), in the
+ * stream format its decoder reads; this encoder's quantiser and the choice of
+ * intra blocks are its own, so streams are valid but not byte-identical to
+ * the reference encoder's.  Host code.  DVC_E_ARG when stream is too short. */
+int dvc_intra_encode_frame(const uint8_t *ori, int width, int height, int intra_qp, const uint8_t *mode,
+                           uint8_t *stream, size_t stream_bytes, size_t *bit_offset, uint8_t *recon,
+                           int *block_bits);
 
 /* Self-check of the belief-propagation magnitude table, host code, no GPU:
  * sweeps phi(y) = -logf(tanhf(y)) with this host's C library over every

@@ -38,7 +38,10 @@ from dvc_b200 import synth  # noqa: E402
 from oracle import refrun  # noqa: E402
 import ladders as lad  # noqa: E402
 
-# name: (kind, frames, gop, qindex, seed[, skip[, intra[, deblock]]])
+# name: (kind, frames, gop, qindex, seed[, skip[, intra[, deblock[, own]]]]); own=1: the
+# bitstreams come from this package's encoder (dvc_b200.encoder, skip and intra
+# decisions of its own) instead of the reference encoder, and are decoded by the
+# reference decoder as usual
 SEQUENCES = {
     "qcif_g2_q4": ("qcif", 5, 2, 4, 11),
     "qcif_g4_q8": ("qcif", 5, 4, 8, 12),
@@ -52,10 +55,13 @@ SEQUENCES = {
     "qcif_g2_q4_full": ("qcif", 5, 2, 4, 11, 1, 1, 1),
     "cif_g4_q6_full": ("cif", 5, 4, 6, 21, 1, 1, 1),
     "qcif_still_g4_q4_full": ("qcif_still", 5, 4, 4, 41, 1, 1, 1),
+    "cif_g4_q4_own_full": ("cif", 9, 4, 4, 21, 1, 1, 1, 1),
+    "qcif_g2_q8_own_full": ("qcif", 5, 2, 8, 12, 1, 1, 1, 1),
+    "qcif_still_g4_q4_own_full": ("qcif_still", 5, 4, 4, 41, 1, 1, 1, 1),
 }
 
 
-def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0, deblock=0):
+def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0, deblock=0, own=0):
     w, h = synth.SHAPES[kind]
     size = "QCIF" if w == 176 else "CIF"
     ori, key = synth.make_sequence(kind, n_frames, seed)
@@ -65,7 +71,14 @@ def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0, deblock=0):
     synth.write_yuv420(oy, ori)
     synth.write_yuv420(ky, key)
     synth.write_frame_stat(st, n_frames)
-    wz, intra_bs, _ = refrun.encode(oy, ky, n_frames, size, gop, q, skip=skip, intra=intra, deblock=deblock)
+    if own:
+        from dvc_b200 import encoder
+        wzb, ib = encoder.encode_sequence_intra(ori, gop, q, 30, deblock, skip, intra)
+        wz, intra_bs = os.path.join(d, "s.wz"), os.path.join(d, "s.intra")
+        open(wz, "wb").write(wzb)
+        open(intra_bs, "wb").write(ib)
+    else:
+        wz, intra_bs, _ = refrun.encode(oy, ky, n_frames, size, gop, q, skip=skip, intra=intra, deblock=deblock)
     cap = os.path.join(d, "cap.bin")
     r = refrun.decode(oy, wz, intra_bs, ky, st, mode=0, capture=cap)
     dec_y = np.frombuffer(r["yuv"], np.uint8).reshape(-1, h, w)
@@ -86,7 +99,7 @@ def run(name, kind, n_frames, gop, q, seed, tmp, skip=0, intra=0, deblock=0):
     frames = sorted(rd)
     np.savez_compressed(
         os.path.join(HERE, f"seq_{name}.npz"),
-        kind=kind, n_frames=n_frames, gop=gop, qindex=q, seed=seed, skip=skip,
+        kind=kind, n_frames=n_frames, gop=gop, qindex=q, seed=seed, skip=skip, own=own,
         wz=np.frombuffer(open(wz, "rb").read(), np.uint8),
         intra=np.frombuffer(open(intra_bs, "rb").read(), np.uint8),
         dec_y=dec_y,

@@ -59,7 +59,7 @@ def test_cli_rejects_bad_arguments(tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("seq", ["qcif_g4_q8", "cif_g2_q2", "qcif_still_g2_q4_skip", "cif_g4_q6_intra",
-                                 "cif_g4_q6_full"])
+                                 "cif_g4_q6_full", "qcif_g2_q8_own_full"])
 def test_cli_decodes_golden_sequence(tmp_path, golden_dir, seq):
     g = dict(np.load(os.path.join(golden_dir, f"seq_{seq}.npz")))
     d, cfg = _setup(tmp_path, g)

@@ -44,3 +44,18 @@ def test_fresh_maps_against_reference_codec():
         n = enc.jbigref_encode(m.ctypes.data_as(C.c_void_p), w, h, out.ctypes.data_as(C.c_void_p), 8192)
         got, used = jbig.decode_mode_map(out[:n].tobytes(), w, h)
         assert used == n and np.array_equal(got, m)
+        # the library's encoder writes the reference encoder's bytes
+        assert jbig.encode_mode_map(m) == out[:n].tobytes()
+
+
+def test_encoder_writes_the_fixture_bytes(golden_dir):
+    g = np.load(os.path.join(golden_dir, "jbig_maps.npz"))
+    for i in range(len(g["used"])):
+        w, h = (int(v) for v in g["sizes"][i])
+        m = g["maps"][g["map_offsets"][i]:g["map_offsets"][i + 1]].reshape(h, w)
+        data = g["data"][g["offsets"][i]:g["offsets"][i + 1]].tobytes()
+        assert jbig.encode_mode_map(m) == data, i
+    # all-zero, all-one and single-pixel maps round-trip through the decoder
+    for m in (np.zeros((36, 44), np.uint8), np.ones((18, 22), np.uint8), np.eye(18, 22, dtype=np.uint8)):
+        got, used = jbig.decode_mode_map(jbig.encode_mode_map(m) + bytes(5), m.shape[1], m.shape[0])
+        assert np.array_equal(got, m) and used == len(jbig.encode_mode_map(m))
