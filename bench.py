@@ -74,15 +74,19 @@ def workload():
 
 def intra_starts(streams, intra_bs, key):
     """Per (GOP, Q): the frames' starting content, key frames with the intra
-    blocks of each WZ frame decoded on the host (dvc_intra_decode_frame)."""
+    blocks of each WZ frame decoded on the host (dvc_intra_decode_frame), the
+    streams on a thread pool (the library call releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
     from dvc_b200 import intra
-    out = {}
-    for gq, st in streams.items():
+
+    def one(gq):
         start = np.array(key, np.uint8, copy=True)
-        for m, (px, _) in intra.decode_all(st, intra_bs[gq], key).items():
+        for m, (px, _) in intra.decode_all(streams[gq], intra_bs[gq], key).items():
             start[m] = px
-        out[gq] = start
-    return out
+        return gq, start
+
+    with ThreadPoolExecutor(max_workers=min(len(streams), os.cpu_count() or 1)) as ex:
+        return dict(ex.map(one, list(streams)))
 
 
 def items(streams, key, starts):

@@ -19,6 +19,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -122,10 +123,28 @@ struct Code {
 };
 using Table = std::vector<Code>;
 
+// a prefix code of length len covers the 16-bit values [lo, hi) whose top
+// len bits are the code: a symbol is found by one binary search on the next 16
+// bits of the stream
+struct Interval {
+  uint32_t lo, hi;
+  int len, sym;
+};
+using Intervals = std::vector<Interval>;
+
 struct Tables {
   Table coeff[3], total_zeros[15], run_before[7];
+  Intervals coeff_iv[3], total_zeros_iv[15], run_before_iv[7];
   bool ok = true;
 };
+
+Intervals intervals(const Table &t) {
+  Intervals v;
+  for (const Code &c : t)
+    v.push_back(Interval{c.bits << (16 - c.len), (c.bits + 1) << (16 - c.len), c.len, c.sym});
+  std::sort(v.begin(), v.end(), [](const Interval &a, const Interval &b) { return a.lo < b.lo; });
+  return v;
+}
 
 void add(Table &t, const char *s, int sym) {
   if (!s || !*s) return;
@@ -151,14 +170,17 @@ const Tables &tables() {
       for (int c = 0; c <= 16; c++)
         for (int t = 0; t < 4; t++) add(T.coeff[v], kCoeffToken[v][c][t], c * 4 + t);
       T.ok = T.ok && prefix_free(T.coeff[v]);
+      T.coeff_iv[v] = intervals(T.coeff[v]);
     }
     for (int i = 0; i < 15; i++) {
       for (int z = 0; z < 16; z++) add(T.total_zeros[i], kTotalZeros[i][z], z);
       T.ok = T.ok && prefix_free(T.total_zeros[i]);
+      T.total_zeros_iv[i] = intervals(T.total_zeros[i]);
     }
     for (int i = 0; i < 7; i++) {
       for (int r = 0; r < 15; r++) add(T.run_before[i], kRunBefore[i][r], r);
       T.ok = T.ok && prefix_free(T.run_before[i]);
+      T.run_before_iv[i] = intervals(T.run_before[i]);
     }
   });
   return T;
@@ -182,16 +204,29 @@ struct Bits {
     for (int i = 0; i < n; i++) v = (v << 1) | (uint32_t)bit();
     return v;
   }
-  int vlc(const Table &t) {
+  // the next 16 bits, zeros past the end
+  uint32_t peek16() const {
     uint32_t v = 0;
-    for (int len = 1; len <= 16; len++) {
-      v = (v << 1) | (uint32_t)bit();
-      if (bad) return -1;
-      for (const Code &c : t)
-        if (c.len == len && c.bits == v) return c.sym;
+    for (int i = 0; i < 16; i++) {
+      const size_t p = pos + (size_t)i;
+      v = (v << 1) | (p < nbits ? (uint32_t)((d[p >> 3] >> (7 - (p & 7))) & 1) : 0u);
     }
-    bad = true;
-    return -1;
+    return v;
+  }
+  int vlc(const Intervals &t) {
+    const uint32_t v = peek16();
+    size_t a = 0, b = t.size();
+    while (a < b) {  // the last interval starting at or below v
+      const size_t m = (a + b) / 2;
+      if (t[m].lo <= v) a = m + 1;
+      else b = m;
+    }
+    if (a == 0 || v >= t[a - 1].hi || pos + (size_t)t[a - 1].len > nbits) {
+      bad = true;
+      return -1;
+    }
+    pos += (size_t)t[a - 1].len;
+    return t[a - 1].sym;
   }
 };
 
@@ -227,7 +262,7 @@ int read_coeffs(Bits &bs, const Frame &F, int bx, int by, std::vector<int> &nnz,
       if (t1 > total) return -1;
     }
   } else {
-    const int sym = bs.vlc(T.coeff[nc < 2 ? 0 : nc < 4 ? 1 : 2]);
+    const int sym = bs.vlc(T.coeff_iv[nc < 2 ? 0 : nc < 4 ? 1 : 2]);
     if (sym < 0) return -1;
     total = sym >> 2;
     t1 = sym & 3;
@@ -258,12 +293,12 @@ int read_coeffs(Bits &bs, const Frame &F, int bx, int by, std::vector<int> &nnz,
   }
   int zeros = 0;
   if (total < 16) {
-    zeros = bs.vlc(T.total_zeros[total - 1]);
+    zeros = bs.vlc(T.total_zeros_iv[total - 1]);
     if (zeros < 0) return -1;
   }
   int left = zeros, i = total - 1;
   while (left > 0 && i > 0) {
-    const int r = bs.vlc(T.run_before[std::min(left, 7) - 1]);
+    const int r = bs.vlc(T.run_before_iv[std::min(left, 7) - 1]);
     if (r < 0 || r > left) return -1;
     run[i] = r;
     left -= r;
