@@ -304,14 +304,10 @@ def main():
                 tickets[srv.submit(it)] = i
             waiting = still
             if srv.poll():
-                for t in list(tickets):
-                    try:
-                        r = srv.result(t)
-                    except native.DvcError:
-                        continue
+                for t in srv.finished():
+                    r = srv.result(t)
                     lat.append(r["latency_ms"])
-                    res[tickets[t]] = r
-                    tickets.pop(t)
+                    res[tickets.pop(t)] = r
                     done += 1
             else:
                 time.sleep(0.0002)

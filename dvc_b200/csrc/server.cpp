@@ -333,6 +333,15 @@ extern "C" int dvc_server_result(dvc_server *S, long long ticket, uint8_t *recon
   return DVC_OK;
 }
 
+extern "C" int dvc_server_finished(dvc_server *S, long long *tickets, int cap, int *count) {
+  if (!S || !count || cap < 0 || (cap > 0 && !tickets)) return DVC_E_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  int n = 0;
+  for (auto it = S->finished.begin(); it != S->finished.end() && n < cap; ++it) tickets[n++] = it->first;
+  *count = n;
+  return DVC_OK;
+}
+
 extern "C" int dvc_server_stats(dvc_server *S, long long *pending, long long *in_flight, size_t *bytes_in_flight) {
   if (!S) return DVC_E_ARG;
   std::lock_guard<std::mutex> lk(S->mu);

@@ -89,6 +89,7 @@ FRAME_API = {
     "dvc_server_result": [C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(C.c_int), C.c_void_p,
                           C.POINTER(C.c_double)],
     "dvc_server_config": [C.c_void_p, C.c_int],
+    "dvc_server_finished": [C.c_void_p, C.POINTER(C.c_longlong), C.c_int, C.POINTER(C.c_int)],
     "dvc_server_stats": [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_size_t)],
     "dvc_ldpca_decode_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
@@ -352,6 +353,13 @@ class Server:
         self.ctx.check(lib().dvc_server_result(self._h, ticket, _ptr(rec), C.byref(bits), _ptr(planes), C.byref(lat)))
         del self._meta[ticket]
         return dict(recon=rec, wz_bits=bits.value, planes=planes, latency_ms=lat.value)
+
+    def finished(self, cap=4096):
+        """Tickets of finished requests not yet collected."""
+        buf = (C.c_longlong * cap)()
+        n = C.c_int(0)
+        self.ctx.check(lib().dvc_server_finished(self._h, buf, cap, C.byref(n)))
+        return [buf[i] for i in range(n.value)]
 
     def stats(self):
         p, f, b = C.c_longlong(0), C.c_longlong(0), C.c_size_t(0)

@@ -243,6 +243,9 @@ int dvc_server_poll(dvc_server *srv, int *completed);
  * latency_ms: from dvc_server_submit to the poll that saw it finished. */
 int dvc_server_result(dvc_server *srv, long long ticket, uint8_t *recon, int *wz_bits, int *plane_results,
                       double *latency_ms);
+/* Tickets of finished requests not yet collected (up to cap of them, oldest
+ * ticket first), so that a caller collects exactly those. */
+int dvc_server_finished(dvc_server *srv, long long *tickets, int cap, int *count);
 int dvc_server_stats(dvc_server *srv, long long *pending, long long *in_flight, size_t *bytes_in_flight);
 /* Dynamic batching window: while another cohort is decoding, a cohort with
  * fewer than max_cohort frames waits up to this long for more (default 2000 us). */

@@ -36,6 +36,7 @@ def test_server_mix_matches_alone(gpu_ctx):
         done += srv.poll()
         time.sleep(0.001)
     assert done == len(mix)
+    assert sorted(srv.finished()) == sorted(tickets)  # every finished ticket listed, none collected yet
     for t, a in zip(tickets, alone):
         r = srv.result(t)
         assert np.array_equal(r["recon"], a["recon"])
@@ -44,6 +45,7 @@ def test_server_mix_matches_alone(gpu_ctx):
         # iterations run, which depends on how widely the ladder was speculated
         assert np.array_equal(r["planes"][:, :3], a["planes"][:, :3])
         assert r["latency_ms"] > 0
+    assert srv.finished() == []
     srv.close()
 
 
