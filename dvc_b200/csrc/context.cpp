@@ -22,6 +22,20 @@ bool DevBuf::ensure(size_t b) {
   return true;
 }
 
+bool DevBuf::ensure(size_t b, cudaStream_t stream) {
+  if (!stream) return ensure(b);
+  if (b <= bytes && p) return true;
+  if (p) cudaFreeAsync(p, stream);
+  p = nullptr;
+  bytes = 0;
+  if (cudaMallocAsync(&p, b ? b : 16, stream) != cudaSuccess) {
+    p = nullptr;
+    return false;
+  }
+  bytes = b;
+  return true;
+}
+
 void DevBuf::release() {
   if (p) cudaFree(p);
   p = nullptr;

@@ -16,6 +16,10 @@ struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
   bool ensure(size_t b);
+  // the same, but a growth frees and allocates in the order of `stream`
+  // (cudaFreeAsync / cudaMallocAsync), without waiting for work on other streams;
+  // for buffers used on that stream only (stream nullptr: as ensure)
+  bool ensure(size_t b, cudaStream_t stream);
   void release();
   template <class T>
   T *as() const { return (T *)p; }

@@ -77,15 +77,16 @@ static cudaError_t ensure_scales() {
   return e;
 }
 
-bool Slot::ensure(int w_, int h_, size_t pdf_floats, size_t in_bytes, size_t out_bytes) {
+bool Slot::ensure(int w_, int h_, size_t pdf_floats, size_t in_bytes, size_t out_bytes, cudaStream_t a) {
   const size_t fs = (size_t)w_ * h_, n = fs / 16;
   const size_t b16n = fs / 256, b8n = fs / 64, octn = (size_t)(w_ - 3) * (h_ - 3) * 16;
-  bool ok = si.ensure(fs) && dbf.ensure(fs) && residue.ensure(fs * 4) && side_trans.ensure(fs * 4) &&
-            recons_trans.ensure(fs * 4) && alpha.ensure(fs * 4) && lr.ensure(n * 4) && oct.ensure(octn * 2) &&
-            smf.ensure(n * 81 * 4) && pdf.ensure(pdf_floats * 4) && mb_mv.ensure(b16n * sizeof(MVd)) &&
-            fmv.ensure(b16n * sizeof(MVd)) && blk_mv.ensure(b8n * sizeof(MVd)) && blk_mv2.ensure(b8n * sizeof(MVd)) &&
-            holes.ensure(b16n * 16) && mse.ensure(b8n * 8) && stats.ensure(32 * 4) && in.ensure(in_bytes) &&
-            out.ensure(out_bytes) && db_img.ensure(fs) && db_mode.ensure(2 * n) && db_bs.ensure(2 * n * 8);
+  bool ok = si.ensure(fs, a) && dbf.ensure(fs, a) && residue.ensure(fs * 4, a) && side_trans.ensure(fs * 4, a) &&
+            recons_trans.ensure(fs * 4, a) && alpha.ensure(fs * 4, a) && lr.ensure(n * 4, a) &&
+            oct.ensure(octn * 2, a) && smf.ensure(n * 81 * 4, a) && pdf.ensure(pdf_floats * 4, a) &&
+            mb_mv.ensure(b16n * sizeof(MVd), a) && fmv.ensure(b16n * sizeof(MVd), a) &&
+            blk_mv.ensure(b8n * sizeof(MVd), a) && blk_mv2.ensure(b8n * sizeof(MVd), a) && holes.ensure(b16n * 16, a) &&
+            mse.ensure(b8n * 8, a) && stats.ensure(32 * 4, a) && in.ensure(in_bytes, a) && out.ensure(out_bytes, a) &&
+            db_img.ensure(fs, a) && db_mode.ensure(2 * n, a) && db_bs.ensure(2 * n * 8, a);
   w = w_;
   h = h_;
   return ok;
@@ -99,6 +100,9 @@ void Slot::release() {
 
 bool FrameBatcher::ensure_pinned(size_t b) {
   if (b <= pinned_bytes_) return true;
+  // grow by at least half (and to 4 MB at first), so that a stream of batches
+  // of changing sizes rarely frees and pins host memory again
+  b = std::max(b, std::max(pinned_bytes_ + pinned_bytes_ / 2, (size_t)4 << 20));
   if (pinned_) cudaFreeHost(pinned_);
   pinned_ = nullptr;
   pinned_bytes_ = 0;
@@ -260,7 +264,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
       memset(P + p.pmode, 0, b8n);
     memcpy(P + p.acc, F.acc, (size_t)qb[f] * nb);
     Slot &S = slots_[f];
-    if (!S.ensure(w, h, (size_t)std::max(nsir, 1) * pdf_stride, p.total, (size_t)qb[f] * 20 + 64))
+    if (!S.ensure(w, h, (size_t)std::max(nsir, 1) * pdf_stride, p.total, (size_t)qb[f] * 20 + 64, alloc_stream_))
       return ctx.fail("device allocation for frame slot failed");
     uint8_t *in = S.in.as<uint8_t>();
     D.mode = in + p.mode;
@@ -311,7 +315,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
   }
   FrameDev *fd_pin = (FrameDev *)(pin + fd_off);
   memcpy(fd_pin, fd.data(), sizeof(FrameDev) * nf);
-  if (!frames_dev_.ensure(sizeof(FrameDev) * nf)) return ctx.fail("device allocation failed");
+  if (!frames_dev_.ensure(sizeof(FrameDev) * nf, alloc_stream_)) return ctx.fail("device allocation failed");
   if (!ctx.cuda_ok(cudaMemcpyAsync(frames_dev_.p, fd_pin, sizeof(FrameDev) * nf, cudaMemcpyHostToDevice, s),
                    "H2D frame descriptors"))
     return false;
@@ -342,7 +346,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
       J.index_in_blk = index;
     }
   }
-  if (!jobs_dev_.ensure(sizeof(LdpcaJob) * std::max<size_t>(1, steps.size() * nf)))
+  if (!jobs_dev_.ensure(sizeof(LdpcaJob) * std::max<size_t>(1, steps.size() * nf), alloc_stream_))
     return ctx.fail("device allocation failed");
   if (!steps.empty() &&
       !ctx.cuda_ok(cudaMemcpyAsync(jobs_dev_.p, jobs, sizeof(LdpcaJob) * steps.size() * nf, cudaMemcpyHostToDevice, s),
@@ -360,7 +364,8 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     int k = std::max(8, sms / std::max(1, std::max(nf, concurrent)));
     if (const char *e = getenv("DVC_LDPCA_SPEC")) k = atoi(e);
     spec_k_ = std::max(1, std::min(32, k));
-    if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_))) return ctx.fail("device allocation failed");
+    if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_), alloc_stream_))
+      return ctx.fail("device allocation failed");
   }
   steps_ = steps;
   fd_ = fd;

@@ -51,7 +51,7 @@ struct Slot {
   DevBuf si, dbf, residue, side_trans, recons_trans, alpha, lr, oct, smf, pdf;
   DevBuf mb_mv, fmv, blk_mv, blk_mv2, holes, mse, stats, in, out;
   DevBuf db_img, db_mode, db_bs;  // deblocking: filtered copy, per-edge mode and strength
-  bool ensure(int w, int h, size_t pdf_floats, size_t in_bytes, size_t out_bytes);
+  bool ensure(int w, int h, size_t pdf_floats, size_t in_bytes, size_t out_bytes, cudaStream_t alloc = nullptr);
   void release();
 };
 
@@ -84,6 +84,9 @@ class FrameBatcher {
               cudaStream_t stream, int max_iter = 50, ProfileStats *prof = nullptr);
   void release();
   size_t slots() const { return slots_.size(); }
+  // grow device buffers in the order of this stream (the batcher is only used
+  // on it), so that a growth does not wait for other streams' work
+  void set_alloc_stream(cudaStream_t s) { alloc_stream_ = s; }
   int frames() const { return nf_; }
   // launches execute() issues (for the launch counter)
   long long launches_per_execute() const;
@@ -91,6 +94,7 @@ class FrameBatcher {
  private:
   std::vector<Slot> slots_;
   DevBuf frames_dev_, jobs_dev_, spec_;
+  cudaStream_t alloc_stream_ = nullptr;
   int spec_k_ = 1;
   void *pinned_ = nullptr;
   size_t pinned_bytes_ = 0;

@@ -225,24 +225,27 @@ static bool start_cohort(dvc_server *S, int i) {
   }
   if ((int)C.out.size() < nf) C.out.resize(nf);
   if (C.pinned_bytes < fs * nf) {
+    // once, for the largest cohort (CIF frames, max_cohort of them): freeing
+    // pinned memory waits for the whole device
+    const size_t most = std::max(fs * nf, (size_t)352 * 288 * S->max_cohort);
     if (C.pinned_out) cudaFreeHost(C.pinned_out);
     C.pinned_out = nullptr;
-    if (cudaMallocHost((void **)&C.pinned_out, fs * nf) != cudaSuccess) return c.fail("pinned allocation failed");
-    C.pinned_bytes = fs * nf;
+    if (cudaMallocHost((void **)&C.pinned_out, most) != cudaSuccess) return c.fail("pinned allocation failed");
+    C.pinned_bytes = most;
   }
   std::vector<dvc::FrameSpec> specs(nf);
   for (int f = 0; f < nf; f++) {
     Request &r = *C.reqs[f];
     for (int k = 0; k < 2; k++) {
       dvc::DevBuf &rb = C.ref[2 * f + k], &lb = C.lp[2 * f + k], &ib = C.ip[2 * f + k];
-      if (!rb.ensure(fs) || !lb.ensure(fs) || !ib.ensure(4 * fs)) return c.fail("device allocation failed");
+      if (!rb.ensure(fs, s) || !lb.ensure(fs, s) || !ib.ensure(4 * fs, s)) return c.fail("device allocation failed");
       const std::vector<uint8_t> &src = k == 0 ? r.past : r.future;
       if (!c.cuda_ok(cudaMemcpyAsync(rb.p, src.data(), fs, cudaMemcpyHostToDevice, s), "H2D reference") ||
           !c.cuda_ok(dvc::launch_ref_planes(rb.as<uint8_t>(), w, h, lb.as<uint8_t>(), ib.as<uint8_t>(), s),
                      "reference planes"))
         return false;
     }
-    if (!C.out[f].ensure(fs)) return c.fail("device allocation failed");
+    if (!C.out[f].ensure(fs, s)) return c.fail("device allocation failed");
     if (!c.cuda_ok(cudaMemcpyAsync(C.out[f].p, r.recon.data(), fs, cudaMemcpyHostToDevice, s), "H2D recon"))
       return false;
     dvc::FrameSpec &sp = specs[f];
@@ -271,6 +274,7 @@ static bool start_cohort(dvc_server *S, int i) {
   }
   int in_flight = 0;
   for (auto &o : S->cohorts) in_flight += (int)o.reqs.size();
+  C.batcher.set_alloc_stream(s);
   if (!C.batcher.prepare(c, specs, s, in_flight) || !C.batcher.execute(c, s, 50, nullptr)) return false;
   for (int f = 0; f < nf; f++)
     if (!c.cuda_ok(cudaMemcpyAsync(C.pinned_out + f * fs, C.out[f].p, fs, cudaMemcpyDeviceToHost, s), "D2H recon"))

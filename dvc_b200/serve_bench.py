@@ -79,6 +79,7 @@ def serve(srv, reqs, arrivals):
     n = len(reqs)
     res, tickets, lat = {}, {}, []
     waiting = list(range(n))
+    host = {"poll_s": 0.0, "poll_max_ms": 0.0, "submit_s": 0.0, "polls": 0}
     t0 = time.perf_counter()
     while len(res) < n:
         now = time.perf_counter() - t0
@@ -93,15 +94,24 @@ def serve(srv, reqs, arrivals):
                 for dep in it["_deps"]:
                     if reqs[dep]["_frame"] == d:
                         sub[name] = res[dep]
+            ts = time.perf_counter()
             tickets[srv.submit(sub)] = k
+            host["submit_s"] += time.perf_counter() - ts
         waiting = still
-        if srv.poll():
+        tp = time.perf_counter()
+        got = srv.poll()
+        tp = time.perf_counter() - tp
+        host["poll_s"] += tp
+        host["poll_max_ms"] = max(host["poll_max_ms"], 1e3 * tp)
+        host["polls"] += 1
+        if got:
             for t in srv.finished():
                 r = srv.result(t)
                 res[tickets.pop(t)] = r["recon"]
                 lat.append(r["latency_ms"])
         else:
             time.sleep(0.0002)
+    serve.host = host
     return time.perf_counter() - t0, lat, res
 
 
@@ -129,7 +139,8 @@ def main():
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
         dt, lat, served = serve(srv, reqs, arrivals)
         sweep.append({"offered_rate": rate, "throughput": n / dt, "requests": n,
-                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "host": dict(serve.host, seconds=dt)})
     srv.close()
     # the plain drop-in on the same requests, in order (references from its own results)
     res_all = {}
