@@ -103,7 +103,10 @@ bool FrameBatcher::ensure_pinned(size_t b) {
   // grow by at least half (and to 4 MB at first), so that a stream of batches
   // of changing sizes rarely frees and pins host memory again
   b = std::max(b, std::max(pinned_bytes_ + pinned_bytes_ / 2, (size_t)4 << 20));
-  if (pinned_) cudaFreeHost(pinned_);
+  // freeing pinned memory waits for the whole device: keep the outgrown
+  // buffer until release() (growth is geometric, so at most about twice the
+  // final size is held)
+  if (pinned_) retired_pinned_.push_back(pinned_);
   pinned_ = nullptr;
   pinned_bytes_ = 0;
   if (cudaMallocHost(&pinned_, b) != cudaSuccess) return false;
@@ -118,7 +121,10 @@ void FrameBatcher::release() {
   slots_.clear();
   frames_dev_.release();
   jobs_dev_.release();
+  spec_.release();
   if (pinned_) cudaFreeHost(pinned_);
+  for (void *p : retired_pinned_) cudaFreeHost(p);
+  retired_pinned_.clear();
   pinned_ = nullptr;
   pinned_bytes_ = 0;
 }

@@ -98,6 +98,7 @@ class FrameBatcher {
   int spec_k_ = 1;
   void *pinned_ = nullptr;
   size_t pinned_bytes_ = 0;
+  std::vector<void *> retired_pinned_;  // outgrown pinned buffers, freed by release()
   bool ensure_pinned(size_t b);
   // prepared state
   struct Step {

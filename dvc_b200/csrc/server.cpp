@@ -118,6 +118,17 @@ extern "C" int dvc_server_create(dvc_ctx *ctx, size_t mem_budget_bytes, int nstr
   S->budget = mem_budget_bytes;
   S->max_cohort = max_cohort;
   S->cohorts.resize(nstreams);
+  // cohort buffers grow with cudaMallocAsync / cudaFreeAsync: keep freed memory
+  // in this process's pool rather than handing it back to the driver at every
+  // synchronisation (a process-local attribute of the current device's pool)
+  {
+    cudaMemPool_t pool;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   for (int i = 0; i < nstreams; i++) {
     cudaStream_t st;
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
