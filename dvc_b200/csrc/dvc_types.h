@@ -52,7 +52,7 @@ struct LdpcaJob {
 // successful code, summed BP iterations and first code; per (codeword, block)
 // the code it succeeded with and its decoded bits.
 struct LdpcaSpec {
-  int *best = nullptr, *iters = nullptr, *start = nullptr, *slot_code = nullptr;
+  int *best = nullptr, *iters = nullptr, *start = nullptr, *done = nullptr, *slot_code = nullptr;
   uint8_t *slot_dec = nullptr;
 };
 

@@ -372,6 +372,8 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     spec_k_ = std::max(1, std::min(32, k));
     if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_), alloc_stream_))
       return ctx.fail("device allocation failed");
+    if (!ctx.cuda_ok(ldpca_spec_reset(ldpca_spec_carve(spec_.p, nf, spec_k_), nf, spec_k_, s), "LDPCA scratch"))
+      return false;
   }
   steps_ = steps;
   fd_ = fd;
@@ -391,8 +393,10 @@ long long FrameBatcher::launches_per_execute() const {
   long long bands = 0;
   for (size_t i = 0; i < steps_.size(); i++)
     if (i == 0 || steps_[i].band != steps_[i - 1].band) bands++;
-  // side info 8, prep 6, per band 1 + 5, per step condBitProb + ladder + finalize, final 1
-  return 8 + 6 + bands * 6 + (long long)steps_.size() * 3 + 1;
+  bool deblock = false;
+  for (const FrameDev &f : fd_) deblock = deblock || f.deblock;
+  // side info 8, prep 6, per band 1 + 5, per step condBitProb + ladder, final 1, deblocking 5
+  return 8 + 6 + bands * 6 + (long long)steps_.size() * 2 + 1 + (deblock ? 5 : 0);
 }
 
 bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileStats *prof) {

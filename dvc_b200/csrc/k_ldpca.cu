@@ -19,9 +19,11 @@
 //    iff BP converges and the CRC matches and no lower code was accepted, i.e.
 //    the accepted code is the lowest code that succeeds; blocks publish
 //    successes with atomicMin, stop at (or abandon) codes above the best success
-//    so far, and ldpca_finalize_kernel picks the lowest success (or the
-//    full-rate inverse when none), so results are identical to the sequential
-//    ladder while idle SMs shorten it.
+//    so far, and the last of the K blocks to finish (a counter with fences)
+//    picks the lowest success (or the full-rate inverse when none), writes the
+//    outputs and resets the codeword's scratch for the next launch, so results
+//    are identical to the sequential ladder while idle SMs shorten it, with one
+//    launch per bitplane step.
 //
 // Edge messages are kept in row order (each row's edges contiguous, in
 // increasing edge index), so a row sum is a sequential pass over contiguous
@@ -366,8 +368,45 @@ __global__ void __launch_bounds__(NT, 1)
     }
   }
   if (spec) {
-    if (tid == 0) atomicAdd(sp.iters + j, total_iters);
-    return;
+    // the last of the codeword's K blocks to finish writes its result: the
+    // lowest successful code (or the full-rate inverse when no code below it
+    // succeeded), then puts the codeword's scratch back to its initial state
+    // for the next launch (no memset between the steps of a batch)
+    __shared__ int s_slot, s_iters;
+    __syncthreads();
+    if (tid == 0) {
+      atomicAdd(sp.iters + j, total_iters);
+      __threadfence();
+      s_stop = atomicAdd(sp.done + j, 1) == K - 1;
+    }
+    __syncthreads();
+    if (!s_stop) return;
+    __threadfence();
+    if (tid == 0) {
+      const int best = __ldcg(sp.best + j);
+      int acc = last, slot = -1;
+      if (best != LDPCA_NONE && best < last)
+        for (int k = 0; k < K; k++)
+          if (__ldcg(sp.slot_code + j * K + k) == best) {
+            slot = k;
+            acc = best;
+          }
+      s_accepted = acc;
+      s_slot = slot;
+      s_iters = __ldcg(sp.iters + j);
+    }
+    __syncthreads();
+    if (s_slot >= 0) {
+      const uint8_t *src = sp.slot_dec + (size_t)(j * K + s_slot) * n;
+      for (int k = tid; k < n; k += NT) dec[k] = __ldcg(src + k);
+    }
+    total_iters = s_iters;
+    for (int k = tid; k < K; k += NT) sp.slot_code[j * K + k] = -1;
+    if (tid == 0) {
+      sp.best[j] = LDPCA_NONE;
+      sp.iters[j] = 0;
+      sp.done[j] = 0;
+    }
   }
   __syncthreads();
   const int accepted = s_accepted;
@@ -384,47 +423,6 @@ __global__ void __launch_bounds__(NT, 1)
   }
   if (J.decoded)
     for (int k = tid; k < n; k += NT) J.decoded[k] = dec[k];
-  if (J.recons_trans) put_bitplane(J, dec, n);
-}
-
-// Speculative form: pick the lowest successful code (or the full-rate inverse
-// when no code below it succeeded) and write the outputs.
-__global__ void __launch_bounds__(256) ldpca_finalize_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, int K,
-                                                             LdpcaSpec sp) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  const int j = blockIdx.x;
-  const LdpcaJob J = jobs[j];
-  if (!J.active) return;
-  const int n = L.n, last = L.num_codes - 1;
-  uint32_t *sw = reinterpret_cast<uint32_t *>(smem);
-  uint8_t *acc = smem + (size_t)((n + 31) / 32) * 4, *synd = acc + n, *dec = synd + n;
-  const int best = sp.best[j];
-  const uint8_t *src = nullptr;
-  int accepted = last;
-  if (best != LDPCA_NONE && best < last) {
-    for (int k = 0; k < K; k++)
-      if (sp.slot_code[j * K + k] == best) src = sp.slot_dec + (size_t)(j * K + k) * n;
-    accepted = best;
-  }
-  if (src) {
-    for (int k = threadIdx.x; k < n; k += blockDim.x) dec[k] = src[k];
-    __syncthreads();
-  } else {
-    accepted = last;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) acc[k] = (uint8_t)((J.acc[k >> 3] >> (7 - (k & 7))) & 1);
-    __syncthreads();
-    build_syndrome(L, last, acc, synd);
-    __syncthreads();
-    invh_decode(L, synd, dec, sw);
-  }
-  if (threadIdx.x == 0) {
-    J.result[0] = L.synd_len[accepted] + 8;
-    J.result[1] = sp.start[j];
-    J.result[2] = accepted;
-    J.result[3] = sp.iters[j];
-  }
-  if (J.decoded)
-    for (int k = threadIdx.x; k < n; k += blockDim.x) J.decoded[k] = dec[k];
   if (J.recons_trans) put_bitplane(J, dec, n);
 }
 
@@ -468,7 +466,7 @@ cudaError_t launch_ldpca(const LadderDev &L, const LdpcaJob *jobs_dev, int num_j
 }
 
 size_t ldpca_spec_scratch_bytes(int n, int num_jobs, int K) {
-  return (size_t)num_jobs * 12 + (size_t)num_jobs * K * 4 + (size_t)num_jobs * K * n + 64;
+  return (size_t)num_jobs * 16 + (size_t)num_jobs * K * 4 + (size_t)num_jobs * K * n + 64;
 }
 
 LdpcaSpec ldpca_spec_carve(void *base, int num_jobs, int K) {
@@ -480,25 +478,27 @@ LdpcaSpec ldpca_spec_carve(void *base, int num_jobs, int K) {
   p += (size_t)num_jobs * 4;
   sp.start = (int *)p;
   p += (size_t)num_jobs * 4;
+  sp.done = (int *)p;
+  p += (size_t)num_jobs * 4;
   sp.slot_code = (int *)p;
   p += (size_t)num_jobs * K * 4;
   sp.slot_dec = p;
   return sp;
 }
 
-cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
-                              int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream) {
-  if (num_jobs <= 0) return cudaSuccess;
+cudaError_t ldpca_spec_reset(const LdpcaSpec &sp, int num_jobs, int K, cudaStream_t stream) {
   cudaError_t e;
   if ((e = cudaMemsetAsync(sp.best, 0x7f, (size_t)num_jobs * 4, stream)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(sp.iters, 0, (size_t)num_jobs * 4, stream)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(sp.slot_code, 0xff, (size_t)num_jobs * K * 4, stream)) != cudaSuccess) return e;
-  e = g_ldpca_threads == 512 ? launch_nt<512>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream)
-                             : launch_nt<1024>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
-  if (e != cudaSuccess) return e;
-  const size_t fsmem = (size_t)((L.n + 31) / 32) * 4 + (size_t)3 * L.n;
-  ldpca_finalize_kernel<<<num_jobs, 256, fsmem, stream>>>(L, jobs_dev, K, sp);
-  return cudaGetLastError();
+  if ((e = cudaMemsetAsync(sp.done, 0, (size_t)num_jobs * 4, stream)) != cudaSuccess) return e;
+  return cudaMemsetAsync(sp.slot_code, 0xff, (size_t)num_jobs * K * 4, stream);
+}
+
+cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
+                              int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream) {
+  if (num_jobs <= 0) return cudaSuccess;
+  return g_ldpca_threads == 512 ? launch_nt<512>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream)
+                                : launch_nt<1024>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
 }
 
 }  // namespace dvc

@@ -12,9 +12,12 @@ size_t ldpca_smem_size(int n, int e);
 // direct form: one block per codeword, no scratch
 cudaError_t launch_ldpca(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
                          int max_iter, cudaStream_t stream);
-// speculative form: K blocks per codeword plus the finalize kernel; scratch from ldpca_spec_carve
+// speculative form: K blocks per codeword, the last of them writes the result;
+// scratch from ldpca_spec_carve, put in its initial state once by
+// ldpca_spec_reset (each launch leaves it so for the next)
 size_t ldpca_spec_scratch_bytes(int n, int num_jobs, int K);
 LdpcaSpec ldpca_spec_carve(void *base, int num_jobs, int K);
+cudaError_t ldpca_spec_reset(const LdpcaSpec &sp, int num_jobs, int K, cudaStream_t stream);
 cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
                               int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream);
 void set_ldpca_threads(int nt);
