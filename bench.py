@@ -219,6 +219,10 @@ def main():
     ap.add_argument("--max-batch", type=int, default=16)
     ap.add_argument("--streams", type=int, default=16)
     args = ap.parse_args()
+    # one hardware queue per CUDA stream (the default 8 makes the 16 decode
+    # streams share queues and wait behind each other's launches); before CUDA
+    # starts, and a value set by the caller wins
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -333,6 +333,9 @@ std::string exe_dir() {
 }  // namespace
 
 int main(int argc, char **argv) {
+  // one hardware queue per CUDA stream (the session decodes on several); set
+  // before the first CUDA call, a value from the environment wins
+  setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0);
   Options o;
   std::string cfg;
   parse_args(argc, argv, o, cfg);

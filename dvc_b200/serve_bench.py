@@ -124,6 +124,10 @@ def main():
     ap.add_argument("--batch-window-us", type=int, default=None)
     ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
+    # one hardware queue per CUDA stream (the default 8 makes the 16 decode
+    # streams share queues and wait behind each other's launches); before CUDA
+    # starts, and a value set by the caller wins
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     from . import native
     t_build = time.perf_counter()
     reqs = build(args.frames)
