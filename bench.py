@@ -257,8 +257,12 @@ def main():
         for i in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            dev_ms.append(ses.run(profile=(i == args.steps - 1)))
+            dev_ms.append(ses.run())
         barrier()
+    # kernel-level figures from one more, untimed run (a profiled run records an
+    # event pair around every LDPCA launch and is not replayed as a graph)
+    flush.zero_()
+    ses.run(profile=True)
     prof = ses.profile()
     from dvc_b200 import replicas
     step_ms = replicas.max_over_ranks(float(np.mean(dev_ms)))
@@ -433,6 +437,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": int(prof["kernel_launches"]) * args.steps,
+            "graph_replays": ses.replays(),
             "ldpca": {"ms_per_launch": ld_avg_ms, "codewords_per_launch": cw_per_launch,
                       "kernel_ms_per_step": prof["ldpca_ms"],
                       "bp_block_iterations_per_step": bp_iters,

@@ -337,7 +337,12 @@ struct dvc_session {
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   std::vector<cudaEvent_t> done;
   dvc::ProfileStats prof;
-  long long runs = 0;
+  long long runs = 0, replays = 0;
+  // the whole run as one CUDA graph, captured on the second unprofiled run and
+  // replayed after that; graph_failed: capture did not work, stay eager
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool graph_failed = false;
 };
 
 static void session_release(dvc_session *S) {
@@ -349,6 +354,10 @@ static void session_release(dvc_session *S) {
   for (cudaEvent_t e : S->batch_done) cudaEventDestroy(e);
   if (S->t0) cudaEventDestroy(S->t0);
   if (S->t1) cudaEventDestroy(S->t1);
+  if (S->graph_exec) cudaGraphExecDestroy(S->graph_exec);
+  if (S->graph) cudaGraphDestroy(S->graph);
+  S->graph_exec = nullptr;
+  S->graph = nullptr;
 }
 
 extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *frames, int max_batch, int nstreams,
@@ -545,16 +554,19 @@ extern "C" int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *f
   return DVC_OK;
 }
 
-extern "C" int dvc_session_run(dvc_session *S, int profile, double *elapsed_ms) {
-  if (!S) return DVC_E_ARG;
+// every operation of one run, forked from streams[0] at `fork` and joined back
+// to it: the batches in level order (a batch waits for the batches it reads),
+// the planes of decoded frames that later levels use as references, and, when
+// `results` is set, the per-bitplane result copies
+static int session_enqueue(dvc_session *S, bool profile, bool results, cudaEvent_t fork) {
   Context &c = S->ctx->c;
   const int ns = (int)S->streams.size();
   const size_t fs = (size_t)S->w * S->h;
   int st;
   cudaStream_t s0 = S->streams[0];
-  if ((st = cuda_status(c, cudaEventRecord(S->t0, s0), "event"))) return st;
+  if ((st = cuda_status(c, cudaEventRecord(fork, s0), "event"))) return st;
   for (int k = 1; k < ns; k++)
-    if ((st = cuda_status(c, cudaStreamWaitEvent(S->streams[k], S->t0, 0), "wait"))) return st;
+    if ((st = cuda_status(c, cudaStreamWaitEvent(S->streams[k], fork, 0), "wait"))) return st;
   for (size_t b = 0; b < S->batches.size(); b++) {
     cudaStream_t sb = S->streams[S->batch_stream[b]];
     for (int d : S->batch_deps[b])
@@ -564,7 +576,6 @@ extern "C" int dvc_session_run(dvc_session *S, int profile, double *elapsed_ms) 
           (st = cuda_status(c, cudaMemcpyAsync(S->out[i].p, S->init[i].p, fs, cudaMemcpyDeviceToDevice, sb), "D2D")))
         return st;
     if (!S->batches[b].execute(c, sb, 50, profile ? &S->prof : nullptr)) return DVC_E_CUDA;
-    // planes of the decoded frames that later levels use as references
     for (int i : S->batch_frames[b]) {
       if (!S->is_ref[i]) continue;
       if ((st = cuda_status(c, dvc::launch_ref_planes(S->out[i].as<uint8_t>(), S->w, S->h, S->olp[i].as<uint8_t>(),
@@ -573,24 +584,77 @@ extern "C" int dvc_session_run(dvc_session *S, int profile, double *elapsed_ms) 
         return st;
       if (profile) S->prof.kernel_launches += 2;  // low-pass and half-pel kernels
     }
+    if (results && !S->batches[b].enqueue_results(c, sb)) return DVC_E_CUDA;
     if ((st = cuda_status(c, cudaEventRecord(S->batch_done[b], sb), "event"))) return st;
   }
   for (int k = 1; k < ns; k++) {
     if ((st = cuda_status(c, cudaEventRecord(S->done[k], S->streams[k]), "event"))) return st;
     if ((st = cuda_status(c, cudaStreamWaitEvent(s0, S->done[k], 0), "wait"))) return st;
   }
-  if ((st = cuda_status(c, cudaEventRecord(S->t1, s0), "event"))) return st;
-  for (size_t b = 0; b < S->batches.size(); b++)
-    if (!S->batches[b].collect(c, S->results[b], S->streams[S->batch_stream[b]])) return DVC_E_CUDA;
-  if ((st = cuda_status(c, cudaEventSynchronize(S->t1), "session run"))) return st;
-  for (int k = 0; k < ns; k++)
-    if ((st = cuda_status(c, cudaStreamSynchronize(S->streams[k]), "session collect"))) return st;
-  if (profile)
-    for (auto &b : S->batches) b.harvest(&S->prof);
+  return DVC_OK;
+}
+
+// capture one run into S->graph_exec; false (and eager runs from then on) if
+// the capture or the instantiation fails
+static bool session_capture(dvc_session *S) {
+  cudaStream_t s0 = S->streams[0];
+  if (cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+  const int st = session_enqueue(S, false, true, S->t0);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s0, &g);
+  if (st != DVC_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return false;
+  }
+  cudaGraphExec_t x = nullptr;
+  if (cudaGraphInstantiate(&x, g, 0) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    cudaGetLastError();
+    return false;
+  }
+  S->graph = g;
+  S->graph_exec = x;
+  return true;
+}
+
+extern "C" int dvc_session_run(dvc_session *S, int profile, double *elapsed_ms) {
+  if (!S) return DVC_E_ARG;
+  Context &c = S->ctx->c;
+  const int ns = (int)S->streams.size();
+  int st;
+  cudaStream_t s0 = S->streams[0];
+  // from the second unprofiled run on, replay the captured graph (the first
+  // run is eager: it sets the kernels' attributes and fills the buffers)
+  if (!profile && S->runs >= 1 && !S->graph_failed && !S->graph_exec && !session_capture(S)) S->graph_failed = true;
+  if (!profile && S->graph_exec) {
+    if ((st = cuda_status(c, cudaEventRecord(S->t0, s0), "event"))) return st;
+    if ((st = cuda_status(c, cudaGraphLaunch(S->graph_exec, s0), "graph launch"))) return st;
+    if ((st = cuda_status(c, cudaEventRecord(S->t1, s0), "event"))) return st;
+    if ((st = cuda_status(c, cudaEventSynchronize(S->t1), "session run"))) return st;
+    for (size_t b = 0; b < S->batches.size(); b++) S->batches[b].read_results(S->results[b]);
+    S->replays++;
+  } else {
+    if ((st = session_enqueue(S, profile != 0, false, S->t0))) return st;
+    if ((st = cuda_status(c, cudaEventRecord(S->t1, s0), "event"))) return st;
+    for (size_t b = 0; b < S->batches.size(); b++)
+      if (!S->batches[b].collect(c, S->results[b], S->streams[S->batch_stream[b]])) return DVC_E_CUDA;
+    if ((st = cuda_status(c, cudaEventSynchronize(S->t1), "session run"))) return st;
+    for (int k = 0; k < ns; k++)
+      if ((st = cuda_status(c, cudaStreamSynchronize(S->streams[k]), "session collect"))) return st;
+    if (profile)
+      for (auto &b : S->batches) b.harvest(&S->prof);
+  }
   float ms = 0;
   cudaEventElapsedTime(&ms, S->t0, S->t1);
   if (elapsed_ms) *elapsed_ms = ms;
   S->runs++;
+  return DVC_OK;
+}
+
+extern "C" int dvc_session_replays(dvc_session *S, long long *replays) {
+  if (!S || !replays) return DVC_E_ARG;
+  *replays = S->replays;
   return DVC_OK;
 }
 

@@ -83,6 +83,7 @@ FRAME_API = {
     "dvc_session_run": [C.c_void_p, C.c_int, C.POINTER(C.c_double)],
     "dvc_session_frame": [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p],
     "dvc_session_profile": [C.c_void_p, C.c_void_p],
+    "dvc_session_replays": [C.c_void_p, C.POINTER(C.c_longlong)],
     "dvc_server_create": [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.POINTER(C.c_void_p)],
     "dvc_server_submit": [C.c_void_p, C.POINTER(WZFrame), C.POINTER(C.c_longlong)],
     "dvc_server_poll": [C.c_void_p, C.POINTER(C.c_int)],
@@ -303,6 +304,12 @@ class Session:
         planes = np.zeros((self.qbits[i], 4), np.int32)
         self.ctx.check(lib().dvc_session_frame(self._h, i, _ptr(rec), C.byref(bits), _ptr(planes)))
         return rec, bits.value, planes
+
+    def replays(self):
+        """Runs so far that replayed the captured CUDA graph."""
+        n = C.c_longlong(0)
+        self.ctx.check(lib().dvc_session_replays(self._h, C.byref(n)))
+        return n.value
 
     def profile(self):
         out = np.zeros(5, np.float64)

@@ -214,8 +214,14 @@ int dvc_session_create(dvc_ctx *ctx, int count, const dvc_wz_frame *frames, int 
                        dvc_session **out);
 /* Decode every frame of the session once; returns when the device is done.
  * *elapsed_ms: device time of the whole run from CUDA events (may be NULL).
- * profile != 0 also times each LDPCA launch (see dvc_session_profile). */
+ * profile != 0 also times each LDPCA launch (see dvc_session_profile).  The
+ * first run issues its work stream by stream; the second unprofiled run
+ * captures that work (every stream, joined) as one CUDA graph and later
+ * unprofiled runs replay it; a profiled run always issues its work directly.
+ * If the capture fails, every run stays direct. */
 int dvc_session_run(dvc_session *ses, int profile, double *elapsed_ms);
+/* How many runs so far replayed the captured graph. */
+int dvc_session_replays(dvc_session *ses, long long *replays);
 /* Results of the last run for frame `index` (any output may be NULL). */
 int dvc_session_frame(dvc_session *ses, int index, uint8_t *recon, int *wz_bits, int *plane_results);
 /* Accumulated profile since creation: [0] LDPCA kernel ms, [1] LDPCA launches,

@@ -57,7 +57,9 @@ def test_first_frame_stages_match_oracle(gpu_ctx, golden_dir, seq):
 def test_session_levels_match_reference(gpu_ctx, golden_dir, seq):
     """A GOP-4 sequence as one device-resident session: frames 1 and 3 of each GOP
     name frame 2's decoded output as their reference (past_from / future_from),
-    so the second level starts on the device without a host round trip; run twice."""
+    so the second level starts on the device without a host round trip; run
+    three times: the first run is eager, the later ones replay the run captured
+    as a CUDA graph, and a profiled run is eager again."""
     g = np.load(os.path.join(golden_dir, f"seq_{seq}.npz"))
     ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
     st = bs.parse_wz(g["wz"].tobytes())
@@ -73,12 +75,13 @@ def test_session_levels_match_reference(gpu_ctx, golden_dir, seq):
     assert any(it.get("past_from") is not None or it.get("future_from") is not None for it in items)
     ses = gpu_ctx.session(items, max_batch=3, streams=2)
     try:
-        for _ in range(2):
-            ses.run()
+        for r in range(4):
+            ses.run(profile=(r == 3))
             for m, i in where.items():
                 rec, bits, planes = ses.frame(i)
                 assert np.array_equal(rec, g["dec_y"][m]), f"frame {m} Y differs"
                 k = list(g["frames"]).index(m)
                 assert bits == g["bits"][k] - st.frames[m].skip_bits - st.frames[m].intra_map_bits
+        assert ses.replays() == 2  # runs 2 and 3 replayed the graph, the profiled run 4 did not
     finally:
         ses.close()
