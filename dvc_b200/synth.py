@@ -41,20 +41,33 @@ def _params(kind):
 
 
 def make_sequence(kind, n_frames, seed):
-    """Return (original, key) luma sequences, uint8 arrays of shape (T, H, W)."""
+    """Return (original, key) luma sequences, uint8 arrays of shape (T, H, W).
+
+    The background is an analytic texture (128 plus six sinusoids) on an
+    unbounded canvas; each frame evaluates it only where it is seen (the
+    translated frame window and the objects' patches), so long sequences with
+    fast motion need no canvas in memory."""
     w, h = SHAPES[kind]
     p = _params(kind)
     rng = np.random.default_rng(seed)
     margin = (p["vel"] + p["ovel"]) * n_frames + 128
     th, tw = h + 2 * margin, w + 2 * margin
-    yy, xx = np.mgrid[0:th, 0:tw].astype(np.float64)
     amps = rng.dirichlet(np.ones(6)) * 80.0
-    tex = np.full((th, tw), 128.0)
+    waves = []
     for a in amps:
         per = rng.uniform(*p["per"])
         ang = rng.uniform(0, np.pi)
         ph = rng.uniform(0, 2 * np.pi)
-        tex += a * np.sin(2 * np.pi * (xx * np.cos(ang) + yy * np.sin(ang)) / per + ph)
+        waves.append((a, per, ang, ph))
+
+    def tex(y0, x0, hh, ww):
+        """Texture over rows y0..y0+hh-1 and columns x0..x0+ww-1 of the canvas."""
+        yy, xx = np.mgrid[y0:y0 + hh, x0:x0 + ww].astype(np.float64)
+        t = np.full((hh, ww), 128.0)
+        for a, per, ang, ph in waves:
+            t += a * np.sin(2 * np.pi * (xx * np.cos(ang) + yy * np.sin(ang)) / per + ph)
+        return t
+
     vx, vy = rng.integers(-p["vel"], p["vel"] + 1, 2)
     objs = []
     for _ in range(p["n_obj"]):
@@ -67,17 +80,19 @@ def make_sequence(kind, n_frames, seed):
             # texture patch the object carries, taken away from the background window
             sx=int(rng.integers(0, tw - size)), sy=int(rng.integers(0, th - size)),
         ))
+    for o in objs:
+        o["patch"] = tex(o["sy"], o["sx"], o["size"], o["size"])
     orig = np.empty((n_frames, h, w), np.uint8)
     key = np.empty((n_frames, h, w), np.uint8)
     for t in range(n_frames):
         ox, oy = margin + vx * t, margin + vy * t
-        f = tex[oy:oy + h, ox:ox + w].copy()
+        f = tex(oy, ox, h, w)
         for o in objs:
             s = o["size"]
             # objects wrap around inside the frame so they never leave it
             x = (o["x"] + o["vx"] * t) % (w - s)
             y = (o["y"] + o["vy"] * t) % (h - s)
-            f[y:y + s, x:x + s] = tex[o["sy"]:o["sy"] + s, o["sx"]:o["sx"] + s]
+            f[y:y + s, x:x + s] = o["patch"]
         f = np.clip(np.rint(f + rng.normal(0.0, p.get("noise", 3.0), f.shape)), 0, 255)
         k = np.clip(np.rint(f + rng.normal(0.0, 2.0, f.shape)), 0, 255)
         orig[t] = f.astype(np.uint8)

@@ -46,7 +46,8 @@ def test_skip_and_deblock_options_match_reference_encoder(tmp_path):
         assert encoder.encode_sequence(ori, gop, q, deblock=1, skip=1) == open(wz, "rb").read()
 
 
-@pytest.mark.parametrize("seq", ["cif_g4_q4_own_full", "qcif_g2_q8_own_full", "qcif_still_g4_q4_own_full"])
+@pytest.mark.parametrize("seq", ["cif_g4_q4_own_full", "qcif_g2_q8_own_full", "qcif_still_g4_q4_own_full",
+                                 "cif_fast_g8_q4_own_full"])
 def test_own_intra_streams_are_reproduced(golden_dir, seq):
     """Streams with this encoder's skip and intra decisions (decoded by the
     reference decoder into the fixture) come out the same again."""
