@@ -898,32 +898,58 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     int part[4] = {0, 0, 0, 0};  // running SADs of candidate rows y-3 .. y (indexed by row & 3)
     double best = 1e300;
     int bi = 0x7fffffff, thr = 0x7fffffff;
-    for (int y0 = 0; y0 < wh; y0 += 4) {
-#pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const int y = y0 + r;
-        if (y < wh) {
-          const uint32_t *rw = row + y * (WS / 4);
-          const uint32_t v = __funnelshift_r(rw[0], rw[1], sh);
-          // window row y is row m of candidate y - m
-          part[(r - 0) & 3] = (int)__vsadu4(v, c0);
-          part[(r - 1) & 3] += (int)__vsadu4(v, c1);
-          part[(r - 2) & 3] += (int)__vsadu4(v, c2);
-          part[(r - 3) & 3] += (int)__vsadu4(v, c3);
-          const int yo = y - 3;
-          if (yo >= 0) {
-            const int sad = part[(r - 3) & 3];
-            if (sad <= thr) {
-              const double cst = (double)sad * __ldg(wt + yo * 65);
-              if (cst < 10000000.0 && cst < best) {  // rows of an item come in increasing index order
-                best = cst;
-                bi = yo * cw + xo;
-                thr = (int)best;
-              }
-            }
-          }
+    // window row y is row m of candidate y - m; candidate y - 3 is complete at row y
+    auto add_row = [&](int y, int slot) {
+      const uint32_t *rw = row + y * (WS / 4);
+      const uint32_t v = __funnelshift_r(rw[0], rw[1], sh);
+      part[slot & 3] = (int)__vsadu4(v, c0);
+      part[(slot - 1) & 3] += (int)__vsadu4(v, c1);
+      part[(slot - 2) & 3] += (int)__vsadu4(v, c2);
+      part[(slot - 3) & 3] += (int)__vsadu4(v, c3);
+    };
+    auto weigh = [&](int yo, int sad) {
+      if (sad <= thr) {
+        const double cst = (double)sad * __ldg(wt + yo * 65);
+        if (cst < 10000000.0 && cst < best) {  // rows of an item come in increasing index order
+          best = cst;
+          bi = yo * cw + xo;
+          thr = (int)best;
         }
       }
+    };
+    // rows 0..2 only start candidates (wh >= 4 always: the window holds the block)
+    add_row(0, 0);
+    add_row(1, 1);
+    add_row(2, 2);
+    int y = 3;
+    for (; y + 3 < wh; y += 4) {  // slots of rows y .. y+3 are 3, 0, 1, 2 (y = 3 mod 4)
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        add_row(y + r, 3 + r);
+        weigh(y + r - 3, part[(3 + r - 3) & 3]);
+      }
+    }
+    for (; y < wh; y++) {  // the last rows; y - 3 mod 4 as above
+      const uint32_t *rw = row + y * (WS / 4);
+      const uint32_t v = __funnelshift_r(rw[0], rw[1], sh);
+      const int q = y & 3;
+      // the same updates with the slot of row y known only at run time
+      int p0 = part[0], p1 = part[1], p2 = part[2], p3 = part[3];
+      const int s0 = (int)__vsadu4(v, c0), s1 = (int)__vsadu4(v, c1), s2 = (int)__vsadu4(v, c2),
+                s3 = (int)__vsadu4(v, c3);
+      // slot q gets s0 (new), q-1 += s1, q-2 += s2, q-3 (= q+1) += s3
+      int n[4] = {p0, p1, p2, p3};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int d = (q - k) & 3;  // 0: new candidate, 1..3: candidates started 1..3 rows ago
+        n[k] = d == 0 ? s0 : d == 1 ? n[k] + s1 : d == 2 ? n[k] + s2 : n[k] + s3;
+      }
+      part[0] = n[0];
+      part[1] = n[1];
+      part[2] = n[2];
+      part[3] = n[3];
+      const int done = (q + 1) & 3;  // slot of candidate y - 3
+      weigh(y - 3, done == 0 ? part[0] : done == 1 ? part[1] : done == 2 ? part[2] : part[3]);
     }
     if (fut) better(bf, jf, best, bi);
     else better(bp, ip, best, bi);
