@@ -223,31 +223,52 @@ __global__ void __launch_bounds__(NT) forward_me_kernel(FrameDev *frames) {
   if (sl < 0) sl = 0;
   if (sr > w - 16) sr = w - 16;
   const int ww = sr - sl + 16, wh = sb - st + 16;  // staged window (<= 80x80)
-  __shared__ uint8_t win[80 * 80];
-  __shared__ uint8_t blk[256];
+  // window rows of 84 bytes in aligned 4-byte words: the window starts at byte
+  // `wo` of each row (w is a multiple of 4, so the words of [sl & ~3, sl + ww)
+  // stay inside the frame row; ww + 3 <= 84); the block's rows four pixels per
+  // word (first pixel lowest)
+  constexpr int WS = 84;
+  __shared__ __align__(16) uint8_t win[80 * WS];
+  __shared__ uint32_t blk4[64];
   __shared__ double sc[NT / 32];
   __shared__ int sidx[NT / 32];
-  for (int k = threadIdx.x; k < ww * wh; k += NT) {
-    const int y = k / ww, x = k - y * ww;
-    win[k] = F.past_lp[(st + y) * w + sl + x];
+  const int wo = sl & 3, nwd = (wo + ww + 3) >> 2;
+  for (int y = threadIdx.x >> 5; y < wh; y += NT / 32) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(F.past_lp + (size_t)(st + y) * w + (sl - wo));
+    uint32_t *dst = reinterpret_cast<uint32_t *>(win + y * WS);
+    for (int x = threadIdx.x & 31; x < nwd; x += 32) dst[x] = __ldg(src + x);
   }
-  for (int k = threadIdx.x; k < 256; k += NT) blk[k] = F.future_lp[(top + (k >> 4)) * w + left + (k & 15)];
+  for (int k = threadIdx.x; k < 64; k += NT)
+    blk4[k] = __ldg(reinterpret_cast<const uint32_t *>(F.future_lp + (size_t)(top + (k >> 2)) * w + left) + (k & 3));
   __syncthreads();
   const int cw = sr - sl + 1, nc = cw * (sb - st + 1);
   double best = 1e300;
   int bi = 0x7fffffff;
+  // candidate c = py * cw + pxo, advanced by NT without a division per candidate
+  const int dq = NT / cw, dr = NT - dq * cw;
+  int py = threadIdx.x / cw, pxo = threadIdx.x - py * cw;
   for (int c = threadIdx.x; c < nc; c += NT) {
-    const int py = c / cw, pxo = c - py * cw;
+    const int X = pxo + wo, sh = (X & 3) * 8;
+    const uint32_t *rb = reinterpret_cast<const uint32_t *>(win) + (X >> 2);
     int sad = 0;
+#pragma unroll 4
     for (int m = 0; m < 16; m++) {
-      const uint8_t *wr = win + (py + m) * ww + pxo;
-      const uint8_t *br = blk + m * 16;
-#pragma unroll
-      for (int n = 0; n < 16; n++) sad += abs((int)br[n] - (int)wr[n]);
+      const uint32_t *r = rb + (py + m) * (WS / 4);
+      const uint32_t w0 = r[0], w1 = r[1], w2 = r[2], w3 = r[3], w4 = r[4];
+      sad += (int)__vsadu4(__funnelshift_r(w0, w1, sh), blk4[4 * m]);
+      sad += (int)__vsadu4(__funnelshift_r(w1, w2, sh), blk4[4 * m + 1]);
+      sad += (int)__vsadu4(__funnelshift_r(w2, w3, sh), blk4[4 * m + 2]);
+      sad += (int)__vsadu4(__funnelshift_r(w3, w4, sh), blk4[4 * m + 3]);
     }
     const double vx = (double)(sl + pxo - left), vy = (double)(st + py - top);
     const double cost = cost_func((double)sad, vx, vy);
     if (cost < 10000000.0) better(best, bi, cost, c);
+    pxo += dr;
+    py += dq;
+    if (pxo >= cw) {
+      pxo -= cw;
+      py++;
+    }
   }
   block_argmin<NT>(best, bi, sc, sidx);
   if (threadIdx.x == 0) {
