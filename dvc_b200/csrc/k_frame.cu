@@ -536,24 +536,39 @@ __global__ void residue_transform_kernel(FrameDev *frames) {
 // noiseParameter, noiseModel.cpp:14-45: band mean and variance of |T| over
 // every 4x4 block.  The variance accumulates squares past 2^24, so each band's
 // sums run sequentially in raster block order, one thread per band.
-__global__ void noise_band_stats_kernel(FrameDev *frames) {
+// The sums stay sequential in block raster order (one thread per band); the
+// block stages 8 block rows of coefficients at a time in shared memory with
+// coalesced loads, so those threads read shared memory instead of waiting on
+// scattered global loads.
+__global__ void __launch_bounds__(256) noise_band_stats_kernel(FrameDev *frames) {
   FrameDev &F = frames[blockIdx.x];
   if (!F.active) return;
+  constexpr int RB = 8;  // block rows per chunk
+  __shared__ int chunk[RB * 4][352];
   const int band = threadIdx.x;
-  if (band >= 16) return;
-  const int index = c_zigzag[band];
+  const int index = c_zigzag[band & 15];
   // bands are coded while Qbits > 0 in zig-zag order; later ones are unused
-  bool coded = true;
-  for (int b = 0; b <= band; b++) coded = coded && F.qbits[c_zigzag[b]] > 0;
-  if (!coded) return;
+  bool active = band < 16;
+  for (int b = 0; active && b <= band; b++) active = F.qbits[c_zigzag[b]] > 0;
   const int w = F.w, b4w = w / 4, b4h = F.h / 4, b4n = b4w * b4h;
   float mean = 0.0f, var = 0.0f;
-  for (int i = 0; i < b4h; i++)
-    for (int j = 0; j < b4w; j++) {
-      const float c = fabsf((float)F.side_trans[(4 * i + (index >> 2)) * w + 4 * j + (index & 3)]);
-      mean += c;
-      var += c * c;
+  for (int i0 = 0; i0 < b4h; i0 += RB) {
+    const int rows = (b4h - i0 < RB ? b4h - i0 : RB) * 4;
+    __syncthreads();
+    for (int k = threadIdx.x; k < rows * w; k += blockDim.x) {
+      const int r = k / w, x = k - r * w;
+      chunk[r][x] = F.side_trans[(4 * i0 + r) * w + x];
     }
+    __syncthreads();
+    if (active)
+      for (int i = 0; i < rows / 4; i++)
+        for (int j = 0; j < b4w; j++) {
+          const float c = fabsf((float)chunk[4 * i + (index >> 2)][4 * j + (index & 3)]);
+          mean += c;
+          var += c * c;
+        }
+  }
+  if (!active) return;
   mean /= (float)b4n;
   var = var / (float)b4n - mean * mean;
   F.band_mean[band] = mean;
@@ -1308,7 +1323,7 @@ cudaError_t launch_side_info(FrameDev *fr, int nf, int w, int h, cudaStream_t s)
 cudaError_t launch_frame_prep(FrameDev *fr, int nf, int w, int h, cudaStream_t s) {
   const int b4n = (w / 4) * (h / 4);
   residue_transform_kernel<<<g2(b4n, 128, nf), 128, 0, s>>>(fr);
-  noise_band_stats_kernel<<<nf, 32, 0, s>>>(fr);
+  noise_band_stats_kernel<<<nf, 256, 0, s>>>(fr);
   noise_alpha_kernel<<<g2(b4n, 128, nf), 128, 0, s>>>(fr);
   over_complete_kernel<<<dim3((w - 3 + 127) / 128, nf, h - 3), 128, 0, s>>>(fr, -1);
   init_ml_kernel<<<g2(b4n, 128, nf), 128, 0, s>>>(fr);
