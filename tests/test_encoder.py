@@ -79,3 +79,20 @@ def test_intra_coder_round_trip():
         m = np.kron(mode.astype(bool), np.ones((8, 8), bool))
         err = np.abs(rec.astype(int) - ori[1].astype(int))[m].mean()
         assert err < 2.0 + qp / 3.0, (qp, err)  # a working quantiser, not only a valid syntax
+
+
+def test_intra_choice_follows_the_rate_comparison():
+    """The intra share grows with QIndex as the WZ rate estimate grows: none of
+    the 8x8 blocks of the moving CIF content at Q2, most of them at Q8; skip
+    blocks are never intra."""
+    ori, _ = synth.make_sequence("cif", 3, 101)
+    share = {}
+    for q in (2, 8):
+        it, coded = encoder.intra_decision(ori[1], ori[0], ori[2], None, q)
+        share[q] = float(it.mean())
+        assert (coded is None) == (not it.any())
+    assert share[2] == 0.0 and share[8] > 0.5
+    skip = np.zeros((36, 44), bool)
+    skip[::2] = True
+    it, _ = encoder.intra_decision(ori[1], ori[0], ori[2], skip, 8)
+    assert not (it & skip).any()
