@@ -239,7 +239,10 @@ void dvc_session_destroy(dvc_session *ses);
  * frame that alone exceeds the budget is refused with DVC_E_NOMEM.  Every
  * stage, including the per-bitplane syndrome-request feedback, stays on the
  * device; the host only submits, polls and collects.  The server must be polled
- * from one thread at a time. */
+ * from one thread at a time.  Cohort buffers grow in stream order
+ * (cudaMallocAsync), and dvc_server_create sets the release threshold of the
+ * current device's default memory pool so that freed memory stays cached in
+ * this process (other users of that pool in the process see the same). */
 typedef struct dvc_server dvc_server;
 int dvc_server_create(dvc_ctx *ctx, size_t mem_budget_bytes, int streams, int max_cohort, dvc_server **out);
 int dvc_server_submit(dvc_server *srv, const dvc_wz_frame *frame, long long *ticket);
