@@ -1149,3 +1149,142 @@ int dvco_decode_wz_frame(const dvco_ladder *L, dvco_frame *f) {
   free(si);
   return 0;
 }
+
+/* ---------------------------------------------------------------- deblocking
+ * deblock, DvcDec/src/deblock.cpp:346-386: edge decisions on the unfiltered
+ * frame (deblock_44_decision, :228-344), edges filtered in place in raster
+ * order, vertical edges (between horizontal neighbours) first
+ * (deblock_filter, :40-226).  type_map: per 8x8 block 0 WZ, 1 intra, 2 skip;
+ * past_mode: the past reference's block modes when it is a WZ frame (NULL
+ * for a key frame, :270-287). */
+static const unsigned char db_alpha[52] = {0,  0,  0,  0,  0,  0,  0,  0,  0,   0,   0,   0,   0,   0,   0,   0,   4,   4,
+                                           5,  6,  7,  8,  9,  10, 12, 13, 15,  17,  20,  22,  25,  28,  32,  36,  40,  45,
+                                           50, 56, 63, 71, 80, 90, 101, 113, 127, 144, 162, 182, 203, 226, 255, 255};
+static const unsigned char db_beta[52] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4,
+                                          6, 6, 7, 7, 8, 8, 9, 9, 10, 10, 11, 11, 12, 12, 13, 13, 14, 14, 15, 15, 16, 16, 17, 17, 18, 18};
+/* the H.264 tc0 table by strength 1..3 (strength 0 and 4 columns unused or equal) */
+static const unsigned char db_tc0[52][5] = {
+    {0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},
+    {0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},{0,0,0,0,0},
+    {0,0,0,0,0},{0,0,0,1,1},{0,0,0,1,1},{0,0,0,1,1},{0,0,0,1,1},{0,0,1,1,1},{0,0,1,1,1},{0,1,1,1,1},
+    {0,1,1,1,1},{0,1,1,1,1},{0,1,1,1,1},{0,1,1,2,2},{0,1,1,2,2},{0,1,1,2,2},{0,1,1,2,2},{0,1,2,3,3},
+    {0,1,2,3,3},{0,2,2,3,3},{0,2,2,4,4},{0,2,3,4,4},{0,2,3,4,4},{0,3,3,5,5},{0,3,4,6,6},{0,3,4,6,6},
+    {0,4,5,7,7},{0,4,5,8,8},{0,4,6,9,9},{0,5,7,10,10},{0,6,8,11,11},{0,6,8,13,13},{0,7,10,14,14},{0,8,11,16,16},
+    {0,9,12,18,18},{0,10,13,20,20},{0,11,15,23,23},{0,13,17,25,25}};
+
+enum { DB_NONE = 0, DB_WZ = 1, DB_ISWZ = 2 };
+
+static int db_iabs(int v) { return v < 0 ? -v : v; }
+static int db_clip3(int lo, int hi, int v) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* one 4x4 block: did any coefficient change its side-information value
+ * (weighted), and is the pixel variance below 50 */
+static void db_block(const uint8_t *rec, const uint8_t *flag, int w, int bx, int by, const double *weight, double *phi,
+                     double *chi) {
+  int sum = 0, sq = 0;
+  *phi = 0.0;
+  for (int m = 0; m < 4; m++)
+    for (int n = 0; n < 4; n++) {
+      const int idx = (by * 4 + m) * w + bx * 4 + n;
+      if (flag[idx]) *phi += weight[m * 4 + n];
+      sum += rec[idx];
+      sq += rec[idx] * rec[idx];
+    }
+  const double var = (double)sq / 16.0 - ((double)sum / 16.0) * ((double)sum / 16.0);
+  *chi = var < 50.0 ? 1.0 : 0.0;
+}
+
+/* deblock_44_decision: filter mode and strength of the edge between blocks 1 and 2 */
+static int db_decide(const uint8_t *rec, const uint8_t *flag, const uint8_t *type_map, const uint8_t *past_mode, int w,
+                     int x1, int y1, int x2, int y2, const double *weight, double *bs) {
+  const int b8w = w / 8;
+  const int t1 = type_map[(y1 >> 1) * b8w + (x1 >> 1)], t2 = type_map[(y2 >> 1) * b8w + (x2 >> 1)];
+  if (t1 == 1 || t2 == 1) {
+    *bs = (t1 == 1 && t2 == 1) ? 3.0 : ((t1 == 0 || t2 == 0) ? 4.0 : 3.0);
+    return DB_ISWZ;
+  }
+  if (t1 == 2 && t2 == 2) {
+    *bs = 0.0;
+    return DB_NONE;
+  }
+  if (t1 == 2 || t2 == 2) {
+    const int sp = t1 == 2 ? (y1 >> 1) * b8w + (x1 >> 1) : (y2 >> 1) * b8w + (x2 >> 1);
+    *bs = past_mode ? (past_mode[sp] == 1 ? 2.0 : 1.0) : 2.0;
+    return DB_ISWZ;
+  }
+  if (t1 == 0 && t2 == 0) {
+    double phi1, chi1, phi2, chi2;
+    db_block(rec, flag, w, x1, y1, weight, &phi1, &chi1);
+    db_block(rec, flag, w, x2, y2, weight, &phi2, &chi2);
+    const double P = 0.9;
+    *bs = 0.14 * (P * ((phi1 + phi2) / 2.0) + (1.0 - P) * ((chi1 + chi2) / 2.0));
+    return *bs > 0.0 ? DB_WZ : DB_NONE;
+  }
+  return DB_NONE;
+}
+
+/* the four pixel lines across one edge; p[k] is the k-th pixel of a line
+ * counted from block 1's far side (p[0..3] block 1, p[4..7] block 2) */
+static void db_filter(int dir, int mode, double bs, uint8_t *img, int w, int x1, int y1, int x2, int y2, int qp,
+                      double pow_qp) {
+  const int step = dir ? w : 1;
+  const int alpha = db_alpha[qp], beta = db_beta[qp];
+  for (int line = 0; line < 4; line++) {
+    uint8_t *P = img + (y1 * 4 + (dir ? 0 : line)) * w + x1 * 4 + (dir ? line : 0);
+    uint8_t *Q = img + (y2 * 4 + (dir ? 0 : line)) * w + x2 * 4 + (dir ? line : 0);
+    const int L3 = P[0], L2 = P[step], L1 = P[2 * step], L0 = P[3 * step];
+    const int R0 = Q[0], R1 = Q[step], R2 = Q[2 * step], R3 = Q[3 * step];
+    if (!(db_iabs(R0 - L0) < alpha && db_iabs(R0 - R1) < beta && db_iabs(L0 - L1) < beta)) continue;
+    const int strong = (mode == DB_ISWZ) ? ((int)bs == 4) : (bs > 0.14 * 0.5);
+    if (mode == DB_WZ && !(bs > 0.0)) continue;
+    if (strong) {
+      const int rl0 = L0 + R0, small_gap = db_iabs(R0 - L0) < ((alpha >> 2) + 2);
+      const int aq = (db_iabs(R0 - R2) < beta) & small_gap, ap = (db_iabs(L0 - L2) < beta) & small_gap;
+      if (ap) {
+        P[3 * step] = (uint8_t)((R1 + ((L1 + rl0) << 1) + L2 + 4) >> 3);
+        P[2 * step] = (uint8_t)((L2 + L1 + rl0 + 2) >> 2);
+        P[step] = (uint8_t)((((L3 + L2) << 1) + L2 + L1 + rl0 + 4) >> 3);
+      } else {
+        P[3 * step] = (uint8_t)(((L1 << 1) + L0 + R1 + 2) >> 2);
+      }
+      if (aq) {
+        Q[0] = (uint8_t)((L1 + ((R1 + rl0) << 1) + R2 + 4) >> 3);
+        Q[step] = (uint8_t)((R2 + R0 + L0 + R1 + 2) >> 2);
+        Q[2 * step] = (uint8_t)((((R3 + R2) << 1) + R2 + R1 + rl0 + 4) >> 3);
+      } else {
+        Q[0] = (uint8_t)(((R1 << 1) + R0 + L1 + 2) >> 2);
+      }
+    } else {
+      const int rl0 = (L0 + R0 + 1) >> 1;
+      const int aq = db_iabs(R0 - R2) < beta, ap = db_iabs(L0 - L2) < beta;
+      const int c0 = mode == DB_ISWZ ? db_tc0[qp][(int)bs] : (int)(bs * (pow_qp - 1));
+      const int tc = c0 + ap + aq;
+      const int dif = db_clip3(-tc, tc, (((R0 - L0) << 2) + (L1 - R1) + 4) >> 3);
+      /* the p1 / q1 updates add to the byte without clipping (it wraps), :186-197 */
+      if (ap) P[2 * step] = (uint8_t)(P[2 * step] + db_clip3(-c0, c0, (L2 + rl0 - (L1 << 1)) >> 1));
+      P[3 * step] = (uint8_t)db_clip3(0, 255, L0 + dif);
+      Q[0] = (uint8_t)db_clip3(0, 255, R0 - dif);
+      if (aq) Q[step] = (uint8_t)(Q[step] + db_clip3(-c0, c0, (R2 + rl0 - (R1 << 1)) >> 1));
+    }
+  }
+}
+
+void dvco_deblock(const uint8_t *recon, const uint8_t *flag, const uint8_t *type_map, const uint8_t *past_mode, int w,
+                  int h, int qindex, int intra_qp, uint8_t *out) {
+  const int b4w = w / 4, b4h = h / 4;
+  double weight[16];
+  int sum = 0;
+  for (int i = 0; i < 16; i++) sum += qtable[qindex][i];
+  for (int i = 0; i < 16; i++) weight[i] = (double)qtable[qindex][i] / (double)sum;
+  const double pow_qp = pow(2, (double)intra_qp / 6.0);
+  memcpy(out, recon, (size_t)w * h);
+  for (int dir = 0; dir < 2; dir++) {
+    const int xd = dir ? 0 : 1, yd = dir ? 1 : 0;
+    for (int i = 0; i < b4h - yd; i++)
+      for (int j = 0; j < b4w - xd; j++) {
+        double bs = 0.0;
+        const int mode = db_decide(recon, flag, type_map, past_mode, w, j, i, j + xd, i + yd, weight, &bs);
+        if (mode == DB_WZ || mode == DB_ISWZ) db_filter(dir, mode, bs, out, w, j, i, j + xd, i + yd, intra_qp, pow_qp);
+      }
+  }
+}

@@ -77,6 +77,10 @@ void dvco_create_side_info(int w, int h, const uint8_t *past, const uint8_t *fut
 void dvco_forward_transform(int w, int h, const int *in, int *out);            /* transform.cpp:153-190 */
 void dvco_over_complete_transform(int w, int h, const uint8_t *pix, int *trans16); /* transform.cpp:275-298 */
 int dvco_qbits_per_block(int qindex);
+/* deblock, DvcDec/src/deblock.cpp:346-386 (type_map per 8x8 block: 0 WZ, 1 intra, 2 skip;
+ * past_mode NULL when the past reference is a key frame) */
+void dvco_deblock(const uint8_t *recon, const uint8_t *flag, const uint8_t *type_map, const uint8_t *past_mode, int w,
+                  int h, int qindex, int intra_qp, uint8_t *out);
 
 #ifdef __cplusplus
 }

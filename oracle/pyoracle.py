@@ -159,6 +159,21 @@ def decode_frame(stream, fr, past, future, recon_init=None, want=()):
     return out
 
 
+def deblock(recon, flag, type_map, past_mode, qindex, intra_qp):
+    """dvco_deblock: the reference's deblocking filter of one frame (deblock.cpp:346-386)."""
+    h, w = recon.shape
+    rec = np.ascontiguousarray(recon, np.uint8)
+    fl = np.ascontiguousarray(flag, np.uint8).reshape(-1)
+    tm = np.ascontiguousarray(type_map, np.uint8).reshape(-1)
+    pm = None if past_mode is None else np.ascontiguousarray(past_mode, np.uint8).reshape(-1)
+    out = np.zeros((h, w), np.uint8)
+    f = lib().dvco_deblock
+    f.restype = None
+    f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    f(_p(rec), _p(fl), _p(tm), _p(pm) if pm is not None else None, w, h, qindex, intra_qp, _p(out))
+    return out
+
+
 def psnr(a, b):
     """frame.cpp:115-124"""
     d = a.astype(np.int64) - b.astype(np.int64)

@@ -60,3 +60,44 @@ def test_oracle_sequence_matches_reference(golden_dir, seq):
     accepted = np.concatenate([res["planes"][m][1] for (m, _, _) in bs.sequence_order(st.n_frames, st.gop)])
     assert np.array_equal(starts, g["ld_start"])
     assert np.array_equal(accepted, g["ld_accepted"])
+
+
+@pytest.mark.skipif(not __import__("oracle.refrun", fromlist=["ref_available"]).ref_available(),
+                    reason="reference build absent")
+@pytest.mark.parametrize("seq", ["qcif_g2_q4_full", "qcif_still_g4_q4_full"])
+def test_oracle_deblocking_matches_reference_filter(golden_dir, seq, tmp_path):
+    """The oracle's deblocking filter against the reference's own, frame by
+    frame: the reference capture decoder records the filter's inputs (frame,
+    change flags, block modes, past reference) and its output."""
+    import struct
+    from oracle import refrun
+    g = load(golden_dir, f"seq_{seq}.npz")
+    ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
+    st = bs.parse_wz(g["wz"].tobytes())
+    oy, ky, sf = str(tmp_path / "o.yuv"), str(tmp_path / "k.yuv"), str(tmp_path / "s.txt")
+    wz, ib = str(tmp_path / "s.wz"), str(tmp_path / "s.intra")
+    synth.write_yuv420(oy, ori)
+    synth.write_yuv420(ky, key)
+    synth.write_frame_stat(sf, int(g["n_frames"]))
+    open(wz, "wb").write(g["wz"].tobytes())
+    open(ib, "wb").write(g["intra"].tobytes())
+    cap = str(tmp_path / "cap.bin")
+    refrun.decode(oy, wz, ib, ky, sf, mode=0, capture=cap)
+    recs = refrun.read_capture(cap)
+    h, w = st.height, st.width
+    checked = 0
+    cur = {}
+    for tag, b in recs:
+        if tag in ("DBIN", "DBFG", "DBMD"):
+            cur[tag] = np.frombuffer(b, np.uint8)
+        elif tag == "DBBG":
+            (cur["begin"],) = struct.unpack("<i", b)
+        elif tag == "DBOU":
+            begin = cur["begin"]
+            past = st.frames.get(begin)
+            out = po.deblock(cur["DBIN"].reshape(h, w), cur["DBFG"], cur["DBMD"],
+                             None if past is None else past.mode, st.qindex, st.intra_qp)
+            assert np.array_equal(out.reshape(-1), np.frombuffer(b, np.uint8)), f"frame {checked}"
+            checked += 1
+            cur = {}
+    assert checked == len(st.frames)
