@@ -1,7 +1,8 @@
 """Test infrastructure: ctypes binding of the C restatement (oracle/_build/liboracle.so)
 and a whole-sequence driver that mirrors the reference's main loop
 (DvcDec/src/main.cpp:118-142, DVC_Decoder.cpp:26-474) for streams without
-intra blocks; used as the checker in tests, smoke() and bench's CPU leg.
+intra blocks (deblocking included); used as the checker in tests, smoke()
+and bench's CPU leg.
 """
 import ctypes as C
 import math
@@ -196,10 +197,13 @@ def decode_sequence(stream, key_frames, ori_frames, key_bits, key_psnr, frames=N
         fr = stream.frames[m]
         if fr.intra_mode:
             raise NotImplementedError("intra blocks need the intra decoder")
-        if stream.deblock:
-            raise NotImplementedError("deblocking filter")
         r = decode_frame(stream, fr, recon[b], recon[e], recon_init=recon[m])
         recon[m] = r["recon"]
+        if stream.deblock:
+            # the filtered frame is the decoded frame and later levels' reference (DVC_Decoder.cpp:429-435)
+            past = stream.frames.get(fr.past)
+            recon[m] = deblock(r["recon"], r["deblock_flag"], fr.mode, None if past is None else past.mode,
+                               stream.qindex, stream.intra_qp)
         bits[m] = fr.skip_bits + fr.intra_map_bits + r["wz_bits"]
         ps[m] = psnr(recon[m], ori_frames[m])
         planes[m] = (r["start"], r["accepted"])

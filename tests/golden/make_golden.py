@@ -58,6 +58,8 @@ SEQUENCES = {
     "cif_g4_q4_own_full": ("cif", 9, 4, 4, 21, 1, 1, 1, 1),
     "qcif_g2_q8_own_full": ("qcif", 5, 2, 8, 12, 1, 1, 1, 1),
     "qcif_still_g4_q4_own_full": ("qcif_still", 5, 4, 4, 41, 1, 1, 1, 1),
+    "qcif_g2_q4_db": ("qcif", 5, 2, 4, 11, 0, 0, 1),
+    "qcif_g4_q6_db": ("qcif", 5, 4, 6, 14, 0, 0, 1),
     "cif_fast_g8_q8_own_full": ("cif_fast", 9, 8, 8, 51, 1, 1, 1, 1),
     "cif_fast_g8_q4_own_full": ("cif_fast", 9, 8, 4, 52, 1, 1, 1, 1),
 }

@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
                                  "qcif_g4_q8_allintra", "qcif_g2_q4_full", "cif_g4_q6_full",
                                  "qcif_still_g4_q4_full", "cif_g4_q4_own_full", "qcif_g2_q8_own_full",
                                  "qcif_still_g4_q4_own_full", "cif_fast_g8_q8_own_full",
-                                 "cif_fast_g8_q4_own_full"])
+                                 "cif_fast_g8_q4_own_full", "qcif_g2_q4_db", "qcif_g4_q6_db"])
 def test_sequence_matches_reference(gpu_ctx, golden_dir, seq):
     g = np.load(os.path.join(golden_dir, f"seq_{seq}.npz"))
     ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))

@@ -42,7 +42,8 @@ def test_crc_and_accumulated_syndrome_round_trip():
     assert acc_code == 0 and start == 0
 
 
-@pytest.mark.parametrize("seq", ["qcif_g2_q4", "qcif_g4_q8", "qcif_g2_q1", "qcif_still_g2_q4_skip"])
+@pytest.mark.parametrize("seq", ["qcif_g2_q4", "qcif_g4_q8", "qcif_g2_q1", "qcif_still_g2_q4_skip", "qcif_g2_q4_db",
+                                 "qcif_g4_q6_db"])
 def test_oracle_sequence_matches_reference(golden_dir, seq):
     g = load(golden_dir, f"seq_{seq}.npz")
     kind = str(g["kind"])
