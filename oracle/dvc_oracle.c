@@ -1288,3 +1288,278 @@ void dvco_deblock(const uint8_t *recon, const uint8_t *flag, const uint8_t *type
       }
   }
 }
+
+/* ---- intra blocks (IntraMode 1): intraRecon, DvcDec/src/intra.cpp:252-268 ----
+ *
+ * CAVLC entropy decoding of the 4x4 luma blocks (vlc.cpp:423-761), restated
+ * from the H.264 syntax (ITU-T H.264 9.2): coeff_token, trailing-one signs,
+ * levels (level_prefix / level_suffix with the adaptive suffix length),
+ * total_zeros and run_before.  The code tables are the standard's tables 9-5
+ * (0 <= nC < 8), 9-9a and 9-10, written as {length, value} pairs; the reference
+ * holds the same tables (vlc.cpp:89-198, 423-470).  Codes are matched bit by
+ * bit: after each bit, every entry of that length is compared. */
+typedef struct {
+  uint8_t len;
+  uint16_t code;
+} vlc_code;
+
+/* coeff_token by nC class (nC < 2, < 4, < 8), [TotalCoeff][TrailingOnes] */
+static const vlc_code ct_tab[3][17][4] = {
+    {{{1, 1}, {0, 0}, {0, 0}, {0, 0}},
+     {{6, 5}, {2, 1}, {0, 0}, {0, 0}},
+     {{8, 7}, {6, 4}, {3, 1}, {0, 0}},
+     {{9, 7}, {8, 6}, {7, 5}, {5, 3}},
+     {{10, 7}, {9, 6}, {8, 5}, {6, 3}},
+     {{11, 7}, {10, 6}, {9, 5}, {7, 4}},
+     {{13, 15}, {11, 6}, {10, 5}, {8, 4}},
+     {{13, 11}, {13, 14}, {11, 5}, {9, 4}},
+     {{13, 8}, {13, 10}, {13, 13}, {10, 4}},
+     {{14, 15}, {14, 14}, {13, 9}, {11, 4}},
+     {{14, 11}, {14, 10}, {14, 13}, {13, 12}},
+     {{15, 15}, {15, 14}, {14, 9}, {14, 12}},
+     {{15, 11}, {15, 10}, {15, 13}, {14, 8}},
+     {{16, 15}, {15, 1}, {15, 9}, {15, 12}},
+     {{16, 11}, {16, 14}, {16, 13}, {15, 8}},
+     {{16, 7}, {16, 10}, {16, 9}, {16, 12}},
+     {{16, 4}, {16, 6}, {16, 5}, {16, 8}}},
+    {{{2, 3}, {0, 0}, {0, 0}, {0, 0}},
+     {{6, 11}, {2, 2}, {0, 0}, {0, 0}},
+     {{6, 7}, {5, 7}, {3, 3}, {0, 0}},
+     {{7, 7}, {6, 10}, {6, 9}, {4, 5}},
+     {{8, 7}, {6, 6}, {6, 5}, {4, 4}},
+     {{8, 4}, {7, 6}, {7, 5}, {5, 6}},
+     {{9, 7}, {8, 6}, {8, 5}, {6, 8}},
+     {{11, 15}, {9, 6}, {9, 5}, {6, 4}},
+     {{11, 11}, {11, 14}, {11, 13}, {7, 4}},
+     {{12, 15}, {11, 10}, {11, 9}, {9, 4}},
+     {{12, 11}, {12, 14}, {12, 13}, {11, 12}},
+     {{12, 8}, {12, 10}, {12, 9}, {11, 8}},
+     {{13, 15}, {13, 14}, {13, 13}, {12, 12}},
+     {{13, 11}, {13, 10}, {13, 9}, {13, 12}},
+     {{13, 7}, {14, 11}, {13, 6}, {13, 8}},
+     {{14, 9}, {14, 8}, {14, 10}, {13, 1}},
+     {{14, 7}, {14, 6}, {14, 5}, {14, 4}}},
+    {{{4, 15}, {0, 0}, {0, 0}, {0, 0}},
+     {{6, 15}, {4, 14}, {0, 0}, {0, 0}},
+     {{6, 11}, {5, 15}, {4, 13}, {0, 0}},
+     {{6, 8}, {5, 12}, {5, 14}, {4, 12}},
+     {{7, 15}, {5, 10}, {5, 11}, {4, 11}},
+     {{7, 11}, {5, 8}, {5, 9}, {4, 10}},
+     {{7, 9}, {6, 14}, {6, 13}, {4, 9}},
+     {{7, 8}, {6, 10}, {6, 9}, {4, 8}},
+     {{8, 15}, {7, 14}, {7, 13}, {5, 13}},
+     {{8, 11}, {8, 14}, {7, 10}, {6, 12}},
+     {{9, 15}, {8, 10}, {8, 13}, {7, 12}},
+     {{9, 11}, {9, 14}, {8, 9}, {8, 12}},
+     {{9, 8}, {9, 10}, {9, 13}, {8, 8}},
+     {{10, 13}, {9, 7}, {9, 9}, {9, 12}},
+     {{10, 9}, {10, 12}, {10, 11}, {10, 10}},
+     {{10, 5}, {10, 8}, {10, 7}, {10, 6}},
+     {{10, 1}, {10, 4}, {10, 3}, {10, 2}}},
+};
+
+/* total_zeros for TotalCoeff 1..15 (row TotalCoeff - 1), [total_zeros] */
+static const vlc_code tz_tab[15][16] = {
+    {{1, 1}, {3, 3}, {3, 2}, {4, 3}, {4, 2}, {5, 3}, {5, 2}, {6, 3}, {6, 2}, {7, 3}, {7, 2}, {8, 3}, {8, 2}, {9, 3}, {9, 2}, {9, 1}},
+    {{3, 7}, {3, 6}, {3, 5}, {3, 4}, {3, 3}, {4, 5}, {4, 4}, {4, 3}, {4, 2}, {5, 3}, {5, 2}, {6, 3}, {6, 2}, {6, 1}, {6, 0}},
+    {{4, 5}, {3, 7}, {3, 6}, {3, 5}, {4, 4}, {4, 3}, {3, 4}, {3, 3}, {4, 2}, {5, 3}, {5, 2}, {6, 1}, {5, 1}, {6, 0}},
+    {{5, 3}, {3, 7}, {4, 5}, {4, 4}, {3, 6}, {3, 5}, {3, 4}, {4, 3}, {3, 3}, {4, 2}, {5, 2}, {5, 1}, {5, 0}},
+    {{4, 5}, {4, 4}, {4, 3}, {3, 7}, {3, 6}, {3, 5}, {3, 4}, {3, 3}, {4, 2}, {5, 1}, {4, 1}, {5, 0}},
+    {{6, 1}, {5, 1}, {3, 7}, {3, 6}, {3, 5}, {3, 4}, {3, 3}, {3, 2}, {4, 1}, {3, 1}, {6, 0}},
+    {{6, 1}, {5, 1}, {3, 5}, {3, 4}, {3, 3}, {2, 3}, {3, 2}, {4, 1}, {3, 1}, {6, 0}},
+    {{6, 1}, {4, 1}, {5, 1}, {3, 3}, {2, 3}, {2, 2}, {3, 2}, {3, 1}, {6, 0}},
+    {{6, 1}, {6, 0}, {4, 1}, {2, 3}, {2, 2}, {3, 1}, {2, 1}, {5, 1}},
+    {{5, 1}, {5, 0}, {3, 1}, {2, 3}, {2, 2}, {2, 1}, {4, 1}},
+    {{4, 0}, {4, 1}, {3, 1}, {3, 2}, {1, 1}, {3, 3}},
+    {{4, 0}, {4, 1}, {2, 1}, {1, 1}, {3, 1}},
+    {{3, 0}, {3, 1}, {1, 1}, {2, 1}},
+    {{2, 0}, {2, 1}, {1, 1}},
+    {{1, 0}, {1, 1}},
+};
+
+/* run_before for zerosLeft 1..6 and > 6 (row min(zerosLeft, 7) - 1), [run_before] */
+static const vlc_code rb_tab[7][15] = {
+    {{1, 1}, {1, 0}},
+    {{1, 1}, {2, 1}, {2, 0}},
+    {{2, 3}, {2, 2}, {2, 1}, {2, 0}},
+    {{2, 3}, {2, 2}, {2, 1}, {3, 1}, {3, 0}},
+    {{2, 3}, {2, 2}, {3, 3}, {3, 2}, {3, 1}, {3, 0}},
+    {{2, 3}, {3, 0}, {3, 1}, {3, 3}, {3, 2}, {3, 5}, {3, 4}},
+    {{3, 7}, {3, 6}, {3, 5}, {3, 4}, {3, 3}, {3, 2}, {3, 1}, {4, 1}, {5, 1}, {6, 1}, {7, 1}, {8, 1}, {9, 1}, {10, 1}, {11, 1}},
+};
+
+typedef struct {
+  const uint8_t *buf;
+  size_t nbits, pos;
+  int bad; /* set when a read runs past the end or a code is not in its table */
+} ib_reader;
+
+static int ib_bit(ib_reader *r) {
+  if (r->pos >= r->nbits) {
+    r->bad = 1;
+    return 0;
+  }
+  const int b = (r->buf[r->pos >> 3] >> (7 - (int)(r->pos & 7))) & 1; /* MSB first, GetBits vlc.cpp:366-401 */
+  r->pos++;
+  return b;
+}
+
+static int ib_bits(ib_reader *r, int n) {
+  int v = 0;
+  for (int i = 0; i < n; i++) v = (v << 1) | ib_bit(r);
+  return v;
+}
+
+/* Index of the entry of tab[0..count) the next bits spell, or -1. */
+static int ib_vlc(ib_reader *r, const vlc_code *tab, int count) {
+  int v = 0;
+  for (int len = 1; len <= 16 && !r->bad; len++) {
+    v = (v << 1) | ib_bit(r);
+    for (int i = 0; i < count; i++)
+      if (tab[i].len == len && tab[i].code == v) return i;
+  }
+  r->bad = 1;
+  return -1;
+}
+
+/* One level (H.264 9.2.2.1; Level_VLC0 / Level_VLCN, vlc.cpp:231-364):
+ * level_prefix zeros, a suffix of levelSuffixSize bits, levelCode, and the
+ * signed level (levelCode + 2) >> 1 for even codes, (-levelCode - 1) >> 1 for
+ * odd ones. */
+static int ib_level(ib_reader *r, int suffix_length, int first_adjust) {
+  int prefix = 0;
+  while (!r->bad && !ib_bit(r)) prefix++;
+  int size = suffix_length;
+  if (prefix == 14 && suffix_length == 0) size = 4;
+  if (prefix >= 15) size = prefix - 3;
+  int code = ((prefix < 15 ? prefix : 15) << suffix_length) + (size ? ib_bits(r, size) : 0);
+  if (prefix >= 15 && suffix_length == 0) code += 15;
+  if (prefix >= 16) code += (1 << (prefix - 3)) - 4096;
+  if (first_adjust) code += 2; /* first non-trailing-one level when TrailingOnes < 3 */
+  return (code & 1) ? (-code - 1) >> 1 : (code + 2) >> 1;
+}
+
+/* residual_block_cavlc of one 4x4 luma block (vlc.cpp:613-761): coefficients
+ * in zig-zag order into scan[16]; returns TotalCoeff. */
+static int ib_block(ib_reader *r, int nc, int scan[16]) {
+  int total, t1;
+  memset(scan, 0, 16 * sizeof(int));
+  if (nc >= 8) { /* 6-bit fixed-length coeff_token: TotalCoeff - 1 and TrailingOnes, 000011 = none */
+    const int v = ib_bits(r, 6);
+    total = (v >> 2) + 1;
+    t1 = v & 3;
+    if (v == 3) total = t1 = 0;
+  } else {
+    const int i = ib_vlc(r, &ct_tab[nc < 2 ? 0 : nc < 4 ? 1 : 2][0][0], 17 * 4);
+    if (i < 0) return 0;
+    total = i / 4;
+    t1 = i % 4;
+  }
+  if (total == 0 || r->bad) return 0;
+  int level[16], run[16];
+  for (int i = 0; i < t1; i++) level[i] = ib_bit(r) ? -1 : 1; /* trailing ones, highest frequency first */
+  int suffix_length = (total > 10 && t1 < 3) ? 1 : 0;
+  for (int i = t1; i < total; i++) {
+    level[i] = ib_level(r, suffix_length, i == t1 && t1 < 3);
+    const int a = level[i] < 0 ? -level[i] : level[i];
+    if (suffix_length == 0) suffix_length = 1;
+    if (a > (3 << (suffix_length - 1)) && suffix_length < 6) suffix_length++;
+  }
+  int zeros_left = 0;
+  if (total < 16) {
+    zeros_left = ib_vlc(r, tz_tab[total - 1], 16);
+    if (zeros_left < 0) return 0;
+  }
+  for (int i = 0; i < total - 1; i++) {
+    run[i] = 0;
+    if (zeros_left > 0) {
+      run[i] = ib_vlc(r, rb_tab[(zeros_left < 7 ? zeros_left : 7) - 1], 15);
+      if (run[i] < 0) return 0;
+    }
+    zeros_left -= run[i];
+  }
+  run[total - 1] = zeros_left;
+  if (zeros_left < 0) {
+    r->bad = 1;
+    return 0;
+  }
+  int pos = -1; /* lowest frequency last: walk back from level[total-1] */
+  for (int i = total - 1; i >= 0; i--) {
+    pos += run[i] + 1;
+    if (pos > 15) {
+      r->bad = 1;
+      return 0;
+    }
+    scan[pos] = level[i];
+  }
+  return total;
+}
+
+/* 4x4 inverse core transform of intra blocks (intra.cpp:35-80): columns
+ * first, then rows, then >> 6 without rounding. */
+static void intra_inverse44(int *b) {
+  int t[16];
+  for (int c = 0; c < 4; c++) {
+    const int x0 = b[c], x1 = b[4 + c], x2 = b[8 + c], x3 = b[12 + c];
+    t[c] = x0 + x1 + x2 + (x3 >> 1);
+    t[4 + c] = x0 + (x1 >> 1) - x2 - x3;
+    t[8 + c] = x0 - (x1 >> 1) - x2 + x3;
+    t[12 + c] = x0 - x1 + x2 - (x3 >> 1);
+  }
+  for (int r = 0; r < 4; r++) {
+    const int *x = t + 4 * r;
+    b[4 * r] = x[0] + x[1] + x[2] + (x[3] >> 1);
+    b[4 * r + 1] = x[0] + (x[1] >> 1) - x[2] - x[3];
+    b[4 * r + 2] = x[0] - (x[1] >> 1) - x[2] + x[3];
+    b[4 * r + 3] = x[0] - x[1] + x[2] - (x[3] >> 1);
+  }
+  for (int i = 0; i < 16; i++) b[i] >>= 6;
+}
+
+int dvco_intra_decode_frame(const uint8_t *buf, size_t nbytes, size_t *bit_offset, int w, int h, int intra_qp,
+                            const uint8_t *mode, uint8_t *recon) {
+  if (!transform_ready) transform_init();
+  const int b4w = w / 4, b4h = h / 4, b8w = w / 8;
+  ib_reader r = {buf, nbytes * 8, *bit_offset, 0};
+  int *nnz = (int *)calloc((size_t)b4w * b4h, sizeof(int));
+  if (!nnz) return -1;
+  const double qstep = pow(2.0, ((double)intra_qp - 4.0) / 6.0); /* intra.cpp:253 */
+#define IS_INTRA(bx, by) (mode[((by) >> 1) * b8w + ((bx) >> 1)] == INTRA_B)
+  for (int by = 0; by < b4h && !r.bad; by++)
+    for (int bx = 0; bx < b4w && !r.bad; bx++) {
+      if (!IS_INTRA(bx, by)) continue;
+      /* neighbours count when they lie in an intra 8x8 block (getNeighbour intra.cpp:83-121) */
+      const int left = bx > 0 && IS_INTRA(bx - 1, by), up = by > 0 && IS_INTRA(bx, by - 1);
+      /* nC (predict_nnz vlc.cpp:564-611) */
+      int nc = 0;
+      if (left) nc += nnz[by * b4w + bx - 1];
+      if (up) nc += nnz[(by - 1) * b4w + bx];
+      if (left && up) nc = (nc + 1) >> 1;
+      int scan[16], blk[16];
+      nnz[by * b4w + bx] = ib_block(&r, nc, scan);
+      /* de-quantisation in double (read_one_block intra.cpp:187-215) */
+      for (int i = 0; i < 16; i++) blk[i] = 0;
+      for (int k = 0; k < 16; k++) blk[zigzag[k]] = scan[k];
+      for (int i = 0; i < 16; i++) blk[i] = ROUND((double)blk[i] * qstep * pre_scale[i]);
+      intra_inverse44(blk);
+      /* DC prediction from the intra neighbours' decoded pixels (intra4x4_dc_pred intra.cpp:124-185) */
+      const int x0 = 4 * bx, y0 = 4 * by;
+      int s = 0;
+      if (up)
+        for (int i = 0; i < 4; i++) s += recon[(y0 - 1) * w + x0 + i];
+      if (left)
+        for (int i = 0; i < 4; i++) s += recon[(y0 + i) * w + x0 - 1];
+      const int dc = (up && left) ? (s + 4) >> 3 : (up || left) ? (s + 2) >> 2 : 128;
+      /* SampleRecon intra.cpp:218-238 */
+      for (int y = 0; y < 4; y++)
+        for (int x = 0; x < 4; x++) {
+          const int v = blk[4 * y + x] + dc;
+          recon[(y0 + y) * w + x0 + x] = (uint8_t)(v < 0 ? 0 : v > 255 ? 255 : v);
+        }
+    }
+#undef IS_INTRA
+  free(nnz);
+  if (r.bad) return -1;
+  *bit_offset = r.pos;
+  return 0;
+}

@@ -12,6 +12,7 @@
  */
 #ifndef DVC_ORACLE_H
 #define DVC_ORACLE_H
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -81,6 +82,14 @@ int dvco_qbits_per_block(int qindex);
  * past_mode NULL when the past reference is a key frame) */
 void dvco_deblock(const uint8_t *recon, const uint8_t *flag, const uint8_t *type_map, const uint8_t *past_mode, int w,
                   int h, int qindex, int intra_qp, uint8_t *out);
+/* intra blocks of one frame, intraRecon DvcDec/src/intra.cpp:252-268: decodes every
+ * 4x4 block of the 8x8 blocks with mode 1 (raster order over the frame's 4x4
+ * blocks) from the sequence's intra bit string buf[nbytes], starting at
+ * *bit_offset, and writes their pixels into recon[w*h]; other pixels are left
+ * alone.  Returns 0 and advances *bit_offset, or -1 when the string ends inside
+ * a block or holds a code that is not in its table. */
+int dvco_intra_decode_frame(const uint8_t *buf, size_t nbytes, size_t *bit_offset, int w, int h, int intra_qp,
+                            const uint8_t *mode, uint8_t *recon);
 
 #ifdef __cplusplus
 }

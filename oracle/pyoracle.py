@@ -1,7 +1,7 @@
 """Test infrastructure: ctypes binding of the C restatement (oracle/_build/liboracle.so)
 and a whole-sequence driver that mirrors the reference's main loop
-(DvcDec/src/main.cpp:118-142, DVC_Decoder.cpp:26-474) for streams without
-intra blocks (deblocking included); used as the checker in tests, smoke()
+(DvcDec/src/main.cpp:118-142, DVC_Decoder.cpp:26-474), intra blocks and
+deblocking included; used as the checker in tests, smoke()
 and bench's CPU leg.
 """
 import ctypes as C
@@ -175,6 +175,21 @@ def deblock(recon, flag, type_map, past_mode, qindex, intra_qp):
     return out
 
 
+def intra_decode_frame(stream, fr, data, bit_offset, recon):
+    """dvco_intra_decode_frame: the intra blocks of WZ frame `fr` from the
+    sequence's intra bit string `data` (uint8 array) at `bit_offset`, written
+    into `recon` ([H, W] uint8, in place); returns the new bit offset."""
+    f = lib().dvco_intra_decode_frame
+    f.restype = C.c_int
+    f.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    assert recon.dtype == np.uint8 and recon.flags.c_contiguous and recon.shape == (stream.height, stream.width)
+    mode = np.ascontiguousarray(fr.mode, np.uint8)
+    off = C.c_size_t(bit_offset)
+    if f(_p(data), data.size, C.byref(off), stream.width, stream.height, stream.intra_qp, _p(mode), _p(recon)) != 0:
+        raise RuntimeError("oracle: intra bit string of frame %d does not decode" % fr.idx)
+    return off.value
+
+
 def psnr(a, b):
     """frame.cpp:115-124"""
     d = a.astype(np.int64) - b.astype(np.int64)
@@ -182,8 +197,14 @@ def psnr(a, b):
     return 0.0 if mse == 0.0 else 10.0 * math.log10(255.0 * 255.0 / mse)
 
 
-def decode_sequence(stream, key_frames, ori_frames, key_bits, key_psnr, frames=None):
-    """Decode every WZ frame of a stream (intra-free) in the reference's order.
+def decode_sequence(stream, key_frames, ori_frames, key_bits, key_psnr, frames=None, intra_bitstream=None):
+    """Decode every WZ frame of a stream in the reference's order.
+
+    intra_bitstream: the sequence's intra bit string (bytes), needed when frames
+    have intra blocks; a frame's intra blocks are decoded into its buffer first
+    and their bits count into its rate (DVC_Decoder.cpp:41-46).  With `frames`,
+    only those frames are WZ-decoded (the intra bit string is still read
+    through every frame, since it is one string in decoding order).
 
     Returns dict(recon[T,H,W], bits{frame}, psnr{frame}, planes{frame: (start, accepted)}).
     """
@@ -191,12 +212,19 @@ def decode_sequence(stream, key_frames, ori_frames, key_bits, key_psnr, frames=N
     recon = key_frames.copy()
     bits, ps, planes = dict(key_bits), dict(key_psnr), {}
     order = bs.sequence_order(stream.n_frames, stream.gop)
+    data = None if intra_bitstream is None else np.frombuffer(bytes(intra_bitstream), np.uint8)
+    off = 0
     for (m, b, e) in order:
+        fr = stream.frames[m]
+        intra_bits = 0
+        if fr.intra_mode:
+            if data is None:
+                raise ValueError("frame %d has intra blocks; pass the intra bit string" % m)
+            before = off
+            off = intra_decode_frame(stream, fr, data, off, recon[m])
+            intra_bits = off - before
         if frames is not None and m not in frames:
             continue
-        fr = stream.frames[m]
-        if fr.intra_mode:
-            raise NotImplementedError("intra blocks need the intra decoder")
         r = decode_frame(stream, fr, recon[b], recon[e], recon_init=recon[m])
         recon[m] = r["recon"]
         if stream.deblock:
@@ -204,7 +232,7 @@ def decode_sequence(stream, key_frames, ori_frames, key_bits, key_psnr, frames=N
             past = stream.frames.get(fr.past)
             recon[m] = deblock(r["recon"], r["deblock_flag"], fr.mode, None if past is None else past.mode,
                                stream.qindex, stream.intra_qp)
-        bits[m] = fr.skip_bits + fr.intra_map_bits + r["wz_bits"]
+        bits[m] = fr.skip_bits + fr.intra_map_bits + r["wz_bits"] + intra_bits
         ps[m] = psnr(recon[m], ori_frames[m])
         planes[m] = (r["start"], r["accepted"])
     return dict(recon=recon, bits=bits, psnr=ps, planes=planes)

@@ -43,15 +43,21 @@ def test_crc_and_accumulated_syndrome_round_trip():
 
 
 @pytest.mark.parametrize("seq", ["qcif_g2_q4", "qcif_g4_q8", "qcif_g2_q1", "qcif_still_g2_q4_skip", "qcif_g2_q4_db",
-                                 "qcif_g4_q6_db"])
+                                 "qcif_g4_q6_db", "qcif_g2_q4_intra", "qcif_g4_q8_allintra", "qcif_g2_q4_full",
+                                 "qcif_still_g4_q4_full", "qcif_g2_q8_own_full", "qcif_still_g4_q4_own_full"])
 def test_oracle_sequence_matches_reference(golden_dir, seq):
+    """Whole sequences through the oracle against the reference decoder's
+    output: pixels, rates, PSNR and every bitplane's first and accepted code;
+    the intra, skip and deblocking fixtures carry the sequence's intra bit
+    string, which the oracle's own CAVLC decoder reads."""
     g = load(golden_dir, f"seq_{seq}.npz")
     kind = str(g["kind"])
     ori, key = synth.make_sequence(kind, int(g["n_frames"]), int(g["seed"]))
     st = bs.parse_wz(g["wz"].tobytes())
     kb = {f: 4000 for f in range(st.n_frames)}
     kp = {f: 40.0 for f in range(st.n_frames)}
-    res = po.decode_sequence(st, key, ori, kb, kp)
+    intra_bs = g["intra"].tobytes() if "intra" in g.files else None
+    res = po.decode_sequence(st, key, ori, kb, kp, intra_bitstream=intra_bs)
     assert np.array_equal(res["recon"], g["dec_y"])
     for f, b, p, wz in zip(g["frames"], g["bits"], g["psnr"], g["is_wz"]):
         if wz:
@@ -102,3 +108,40 @@ def test_oracle_deblocking_matches_reference_filter(golden_dir, seq, tmp_path):
             checked += 1
             cur = {}
     assert checked == len(st.frames)
+
+
+class _Geom:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+@pytest.mark.parametrize("qp", [0, 12, 30, 51])
+@pytest.mark.parametrize("content", ["noise", "ramp", "half_intra"])
+def test_oracle_intra_reads_encoder_blocks(qp, content):
+    """The oracle's CAVLC reader on intra blocks written by the library's
+    encoder (dvc_intra_encode_frame): every bit consumed and every intra pixel
+    equal to the reconstruction the encoder reports.  IntraQP 0 on noise takes
+    the level_prefix 15 escape (about 4,500 times in the frame) and the 6-bit
+    coeff_token of nC >= 8 (about 1,600 blocks); IntraQP 51 leaves mostly empty
+    blocks."""
+    from dvc_b200 import intra
+    rng = np.random.default_rng(qp * 7 + len(content))
+    h, w = 144, 176
+    if content == "noise":
+        ori = rng.integers(0, 256, (h, w), dtype=np.uint8)
+    else:
+        ori = np.clip(128 + np.cumsum(rng.integers(-9, 10, (h, w)), axis=1), 0, 255).astype(np.uint8)
+    mode = np.ones((h // 8, w // 8), np.uint8) if content != "half_intra" else \
+        (rng.random((h // 8, w // 8)) < 0.5).astype(np.uint8)
+    buf = np.zeros(1 << 20, np.uint8)
+    end, rec = intra.encode_frame(ori, mode, qp, buf, 5)  # a string that starts mid-byte
+    data = buf[:(end + 7) // 8].copy()
+    out = np.zeros((h, w), np.uint8)
+    geom = _Geom(width=w, height=h, intra_qp=qp)
+    fr = _Geom(mode=mode.reshape(-1), idx=1)
+    assert po.intra_decode_frame(geom, fr, data, 5, out) == end
+    px = np.kron(mode, np.ones((8, 8), np.uint8)).astype(bool)
+    assert np.array_equal(out[px], rec[px])
+    assert not out[~px].any()  # pixels of other blocks are left alone
+    with pytest.raises(RuntimeError):  # a string cut short inside the last block
+        po.intra_decode_frame(geom, fr, data[:max(1, (end - 40) // 8)], 5, np.zeros((h, w), np.uint8))
