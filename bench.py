@@ -72,21 +72,34 @@ def workload():
     return ori, key, streams, intra_bs
 
 
+class Starts:
+    """Frame index -> starting content of one stream: the key-frame content
+    with the frame's intra blocks decoded over it for frames that have intra
+    blocks, the key-frame content itself (a view, nothing to decode) for the
+    others."""
+
+    def __init__(self, key, decoded):
+        self.key, self.decoded = key, decoded
+
+    def __getitem__(self, m):
+        px = self.decoded.get(m)
+        return self.key[m] if px is None else px
+
+
 def intra_starts(streams, intra_bs, key):
-    """Per (GOP, Q): the frames' starting content, key frames with the intra
-    blocks of each WZ frame decoded on the host (dvc_intra_decode_frame), the
-    streams on a thread pool (the library call releases the GIL)."""
+    """Per (GOP, Q): the frames' starting content (Starts), the intra blocks of
+    each WZ frame decoded on the host (dvc_intra_decode_frame); the streams on
+    a thread pool (the library call releases the GIL), the longest intra bit
+    strings first."""
     from concurrent.futures import ThreadPoolExecutor
     from dvc_b200 import intra
 
     def one(gq):
-        start = np.array(key, np.uint8, copy=True)
-        for m, (px, _) in intra.decode_all(streams[gq], intra_bs[gq], key).items():
-            start[m] = px
-        return gq, start
+        return gq, Starts(key, {m: px for m, (px, _) in intra.decode_all(streams[gq], intra_bs[gq], key).items()})
 
+    order = sorted(streams, key=lambda gq: -len(intra_bs[gq]))
     with ThreadPoolExecutor(max_workers=min(len(streams), os.cpu_count() or 1)) as ex:
-        return dict(ex.map(one, list(streams)))
+        return dict(ex.map(one, order))
 
 
 def items(streams, key, starts):

@@ -14,7 +14,12 @@
 //
 // The VLC tables are the standard's (ITU-T H.264 tables 9-5, 9-7 and 9-10,
 // luma 4x4); they are written here as code strings and turned into prefix
-// codes at first use, where they are checked to be prefix-free.
+// codes at first use, where they are checked to be prefix-free.  The decoder
+// reads through a 64-bit window of the stream: symbols by direct lookup on
+// its next 10 bits (a binary search for the coeff_tokens longer than that),
+// level prefixes by counting leading zeros; only the coded coefficients are
+// de-quantised, and a block whose only coefficient is the DC skips the
+// transform (its 16 outputs all equal DC >> 6).
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -132,11 +137,35 @@ struct Interval {
 };
 using Intervals = std::vector<Interval>;
 
+// direct lookup on the next `bits` bits of the stream: entry = sym << 8 | len
+// for every value whose top bits are a code of at most `bits` bits, 0 for the
+// rest (a longer code, found by the binary search, or no code at all)
+struct Lut {
+  int bits = 0;
+  std::vector<uint32_t> e;
+};
+
+constexpr int kLutMaxBits = 10;
+
 struct Tables {
   Table coeff[3], total_zeros[15], run_before[7];
   Intervals coeff_iv[3], total_zeros_iv[15], run_before_iv[7];
+  Lut coeff_lut[3], total_zeros_lut[15], run_before_lut[7];
   bool ok = true;
 };
+
+Lut lut(const Table &t) {
+  Lut L;
+  for (const Code &c : t) L.bits = std::max(L.bits, c.len);
+  L.bits = std::min(L.bits, kLutMaxBits);
+  L.e.assign((size_t)1 << L.bits, 0u);
+  for (const Code &c : t) {
+    if (c.len > L.bits) continue;
+    const uint32_t lo = c.bits << (L.bits - c.len), hi = (c.bits + 1) << (L.bits - c.len);
+    for (uint32_t v = lo; v < hi; v++) L.e[v] = ((uint32_t)c.sym << 8) | (uint32_t)c.len;
+  }
+  return L;
+}
 
 Intervals intervals(const Table &t) {
   Intervals v;
@@ -171,62 +200,75 @@ const Tables &tables() {
         for (int t = 0; t < 4; t++) add(T.coeff[v], kCoeffToken[v][c][t], c * 4 + t);
       T.ok = T.ok && prefix_free(T.coeff[v]);
       T.coeff_iv[v] = intervals(T.coeff[v]);
+      T.coeff_lut[v] = lut(T.coeff[v]);
     }
     for (int i = 0; i < 15; i++) {
       for (int z = 0; z < 16; z++) add(T.total_zeros[i], kTotalZeros[i][z], z);
       T.ok = T.ok && prefix_free(T.total_zeros[i]);
       T.total_zeros_iv[i] = intervals(T.total_zeros[i]);
+      T.total_zeros_lut[i] = lut(T.total_zeros[i]);
     }
     for (int i = 0; i < 7; i++) {
       for (int r = 0; r < 15; r++) add(T.run_before[i], kRunBefore[i][r], r);
       T.ok = T.ok && prefix_free(T.run_before[i]);
       T.run_before_iv[i] = intervals(T.run_before[i]);
+      T.run_before_lut[i] = lut(T.run_before[i]);
     }
   });
   return T;
 }
 
+// MSB-first reader over a 64-bit window: window() holds the stream's bits from
+// pos on (at least 57 of them), zeros past the end; consuming bits past the
+// end marks the read bad
 struct Bits {
   const uint8_t *d;
   size_t nbits, pos;
   bool bad = false;
-  int bit() {
-    if (pos >= nbits) {
-      bad = true;
-      return 0;
+  uint64_t window() const {
+    const size_t byte = pos >> 3, nbytes = nbits >> 3;
+    uint64_t w = 0;
+    if (byte + 8 <= nbytes) {
+      memcpy(&w, d + byte, 8);
+      w = __builtin_bswap64(w);
+    } else {
+      for (size_t i = 0; i < 8 && byte + i < nbytes; i++) w |= (uint64_t)d[byte + i] << (56 - 8 * i);
     }
-    const int b = (d[pos >> 3] >> (7 - (pos & 7))) & 1;
-    pos++;
-    return b;
+    return w << (pos & 7);
   }
+  void skip(int n) {
+    pos += (size_t)n;
+    if (pos > nbits) bad = true;
+  }
+  // the next n bits (1 <= n <= 32)
   uint32_t read(int n) {
-    uint32_t v = 0;
-    for (int i = 0; i < n; i++) v = (v << 1) | (uint32_t)bit();
+    const uint32_t v = (uint32_t)(window() >> (64 - n));
+    skip(n);
     return v;
   }
-  // the next 16 bits, zeros past the end
-  uint32_t peek16() const {
-    uint32_t v = 0;
-    for (int i = 0; i < 16; i++) {
-      const size_t p = pos + (size_t)i;
-      v = (v << 1) | (p < nbits ? (uint32_t)((d[p >> 3] >> (7 - (p & 7))) & 1) : 0u);
+  int bit() { return (int)read(1); }
+  // one symbol of a prefix code: the lookup table, else the binary search
+  // over the next 16 bits
+  int vlc(const Lut &L, const Intervals &t) {
+    const uint64_t w = window();
+    const uint32_t e = L.e[(size_t)(w >> (64 - L.bits))];
+    if (e) {
+      skip((int)(e & 0xFF));
+      return bad ? -1 : (int)(e >> 8);
     }
-    return v;
-  }
-  int vlc(const Intervals &t) {
-    const uint32_t v = peek16();
+    const uint32_t v = (uint32_t)(w >> 48);
     size_t a = 0, b = t.size();
     while (a < b) {  // the last interval starting at or below v
       const size_t m = (a + b) / 2;
       if (t[m].lo <= v) a = m + 1;
       else b = m;
     }
-    if (a == 0 || v >= t[a - 1].hi || pos + (size_t)t[a - 1].len > nbits) {
+    if (a == 0 || v >= t[a - 1].hi) {
       bad = true;
       return -1;
     }
-    pos += (size_t)t[a - 1].len;
-    return t[a - 1].sym;
+    skip(t[a - 1].len);
+    return bad ? -1 : t[a - 1].sym;
   }
 };
 
@@ -236,10 +278,10 @@ struct Frame {
   bool intra(int bx, int by) const { return mode[(by >> 1) * b8w + (bx >> 1)] == 1; }
 };
 
-// levels of one block in scan order into coeff (zig-zag positions); returns
-// the total coefficient count, -1 on a bitstream error
-int read_coeffs(Bits &bs, const Frame &F, int bx, int by, std::vector<int> &nnz, int coeff[16]) {
-  const Tables &T = tables();
+// the coefficients of one block: level lev[k] at block position at[k] (the
+// zig-zag scan mapped to raster order), k < the returned total coefficient
+// count; -1 on a bitstream error
+int read_coeffs(Bits &bs, const Tables &T, const Frame &F, int bx, int by, int *nnz, int at[16], int lev[16]) {
   int nc = 0, cnt = 0;
   if (bx > 0 && F.intra(bx - 1, by)) {
     nc += nnz[by * F.b4w + bx - 1];
@@ -262,27 +304,30 @@ int read_coeffs(Bits &bs, const Frame &F, int bx, int by, std::vector<int> &nnz,
       if (t1 > total) return -1;
     }
   } else {
-    const int sym = bs.vlc(T.coeff_iv[nc < 2 ? 0 : nc < 4 ? 1 : 2]);
+    const int cls = nc < 2 ? 0 : nc < 4 ? 1 : 2;
+    const int sym = bs.vlc(T.coeff_lut[cls], T.coeff_iv[cls]);
     if (sym < 0) return -1;
     total = sym >> 2;
     t1 = sym & 3;
   }
   nnz[by * F.b4w + bx] = total;
-  memset(coeff, 0, 16 * sizeof(int));
   if (total == 0) return 0;
-  int level[16] = {0}, run[16] = {0};
+  int level[16], run[16] = {0};
   // trailing ones, highest frequency first
   for (int k = total - 1; k >= total - t1; k--) level[k] = bs.bit() ? -1 : 1;
   int suffix_len = (total > 10 && t1 < 3) ? 1 : 0;
   for (int k = total - 1 - t1; k >= 0; k--) {
-    int prefix = 0;
-    while (!bs.bit()) {
-      if (bs.bad || ++prefix > 15) return -1;
-    }
+    // level_prefix: the zeros before the next 1 (at most 25 here, which keeps
+    // the prefix, its 1 and a suffix of prefix - 3 bits inside the window)
+    const uint64_t w = bs.window();
+    const int prefix = w ? __builtin_clzll(w) : 64;
+    if (prefix > 25) return -1;
+    bs.skip(prefix + 1);
     int code = (std::min(15, prefix) << suffix_len);
     const int ssize = (prefix == 14 && suffix_len == 0) ? 4 : (prefix >= 15 ? prefix - 3 : suffix_len);
     if (ssize > 0) code += (int)bs.read(ssize);
     if (prefix >= 15 && suffix_len == 0) code += 15;
+    if (prefix >= 16) code += (1 << (prefix - 3)) - 4096;  // escapes beyond 15 (Level_VLC0/VLCN vlc.cpp:231-364)
     if (k == total - 1 - t1 && t1 < 3) code += 2;
     const int v = (code % 2 == 0) ? (code + 2) >> 1 : (-code - 1) >> 1;
     level[k] = v;
@@ -293,12 +338,13 @@ int read_coeffs(Bits &bs, const Frame &F, int bx, int by, std::vector<int> &nnz,
   }
   int zeros = 0;
   if (total < 16) {
-    zeros = bs.vlc(T.total_zeros_iv[total - 1]);
+    zeros = bs.vlc(T.total_zeros_lut[total - 1], T.total_zeros_iv[total - 1]);
     if (zeros < 0) return -1;
   }
   int left = zeros, i = total - 1;
   while (left > 0 && i > 0) {
-    const int r = bs.vlc(T.run_before_iv[std::min(left, 7) - 1]);
+    const int rb = std::min(left, 7) - 1;
+    const int r = bs.vlc(T.run_before_lut[rb], T.run_before_iv[rb]);
     if (r < 0 || r > left) return -1;
     run[i] = r;
     left -= r;
@@ -309,7 +355,8 @@ int read_coeffs(Bits &bs, const Frame &F, int bx, int by, std::vector<int> &nnz,
   for (int k = 0; k < total; k++) {
     pos += run[k];
     if (pos > 15) return -1;
-    coeff[kZigzag[pos]] = level[k];
+    at[k] = kZigzag[pos];
+    lev[k] = level[k];
     pos++;
   }
   return bs.bad ? -1 : total;
@@ -528,20 +575,23 @@ extern "C" int dvc_intra_decode_frame(const uint8_t *stream, size_t stream_bytes
   if (!stream || !bit_offset || !mode || !recon || !((width == 176 && height == 144) || (width == 352 && height == 288)) ||
       intra_qp < 0 || intra_qp > 51)
     return DVC_E_ARG;
-  if (!tables().ok) return DVC_E_DATA;
+  const Tables &T = tables();
+  if (!T.ok) return DVC_E_DATA;
   Frame F{width, height, width / 4, height / 4, width / 8, mode};
   Bits bs{stream, stream_bytes * 8, *bit_offset};
   // de-quantisation scale: Qstep * 64 * pre-scale (intra.cpp:214, transform.cpp:12-52)
   const double qstep = pow(2.0, ((double)intra_qp - 4.0) / 6.0);
   const double a2 = 0.25, b2 = 0.4, ab = 0.5 * sqrt(0.4);
   const double pre[16] = {a2, ab, a2, ab, ab, b2, ab, b2, a2, ab, a2, ab, ab, b2, ab, b2};
+  double pre64[16];
+  for (int i = 0; i < 16; i++) pre64[i] = pre[i] * 64.0;
   std::vector<int> nnz((size_t)F.b4w * F.b4h, 0);
   for (int by = 0; by < F.b4h; by++)
     for (int bx = 0; bx < F.b4w; bx++) {
       if (!F.intra(bx, by)) continue;
-      int coeff[16], blk[16];
-      if (read_coeffs(bs, F, bx, by, nnz, coeff) < 0) return DVC_E_DATA;
-      for (int i = 0; i < 16; i++) blk[i] = round_half_away((double)coeff[i] * qstep * (pre[i] * 64.0));
+      int at[16], lev[16];
+      const int total = read_coeffs(bs, T, F, bx, by, nnz.data(), at, lev);
+      if (total < 0) return DVC_E_DATA;
       // DC prediction from intra neighbours (intra.cpp:120-184)
       const int top = by * 4, left = bx * 4;
       const bool up = by > 0 && F.intra(bx, by - 1), lf = bx > 0 && F.intra(bx - 1, by);
@@ -551,6 +601,19 @@ extern "C" int dvc_intra_decode_frame(const uint8_t *stream, size_t stream_bytes
       if (lf)
         for (int i = 0; i < 4; i++) s += recon[(top + i) * width + left - 1];
       const int pred = (up && lf) ? (s + 4) >> 3 : (up || lf) ? (s + 2) >> 2 : 128;
+      // de-quantisation of the coded coefficients (the others stay 0)
+      int blk[16] = {0};
+      bool dc_only = true;
+      for (int k = 0; k < total; k++) {
+        blk[at[k]] = round_half_away((double)lev[k] * qstep * pre64[at[k]]);
+        dc_only = dc_only && at[k] == 0;
+      }
+      if (dc_only) {  // no residual, or a lone DC: all 16 outputs of the transform equal blk[0] >> 6
+        const int v = (blk[0] >> 6) + pred;
+        const int c = v < 0 ? 0 : v > 255 ? 255 : v;
+        for (int i = 0; i < 4; i++) memset(recon + (size_t)(top + i) * width + left, c, 4);
+        continue;
+      }
       inverse44(blk);
       for (int i = 0; i < 4; i++)
         for (int j = 0; j < 4; j++) {
