@@ -125,6 +125,59 @@ def items(streams, key, starts):
     return out, level, src
 
 
+def serve(srv, its, pool=None, arrivals=None, poll_every=16):
+    """Decode session-style items through a server (native.Server) and poll to
+    completion.  pool None: every item, each submitted as soon as the items it
+    references (past_from / future_from) are done, their decoded frames passed
+    as its references; else request k is item pool[k % len(pool)] (items
+    without references), submitted once arrivals[k] seconds have passed.
+    During a burst of submissions the server is also polled after every
+    `poll_every` of them, so that cohorts start while the rest are still being
+    submitted.  Returns (seconds, latencies in ms, results by item)."""
+    n_req = len(its) if pool is None else len(arrivals)
+    tickets, lat, res = {}, [], {}
+    waiting = list(range(n_req))
+    done = 0
+
+    def pump():
+        """One poll; collects every ticket finished so far.  False when the poll finished nothing."""
+        nonlocal done
+        if not srv.poll():
+            return False
+        for t in srv.finished():
+            r = srv.result(t)
+            lat.append(r["latency_ms"])
+            res[tickets.pop(t)] = r
+            done += 1
+        return True
+
+    t0 = time.perf_counter()
+    while done < n_req:
+        now = time.perf_counter() - t0
+        still, burst = [], 0
+        for k in waiting:
+            i = k if pool is None else pool[k % len(pool)]
+            it = its[i]
+            deps = [it.get("past_from"), it.get("future_from")]
+            if (arrivals is not None and arrivals[k] > now) or any(d is not None and d not in res for d in deps):
+                still.append(k)
+                continue
+            if deps[0] is not None or deps[1] is not None:
+                it = dict(it)
+                for name, d in zip(("past", "future"), deps):
+                    if d is not None:
+                        it[name] = res[d]["recon"]
+                        it.pop(name + "_from")
+            tickets[srv.submit(it)] = i
+            burst += 1
+            if burst % poll_every == 0:
+                pump()
+        waiting = still
+        if not pump():
+            time.sleep(0.0002)
+    return time.perf_counter() - t0, lat, res
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -298,41 +351,7 @@ def main():
     level0 = [i for i in range(len(its)) if lev[i] == 0]
 
     def serve_all(pool=None, arrivals=None):
-        """Submit the items of `pool` at the given offsets in seconds (pool None:
-        every item, each as soon as the items it references are done) and poll
-        to completion.  Returns (seconds, latencies in ms, results by item)."""
-        n_req = len(its) if pool is None else len(arrivals)
-        tickets, lat, res = {}, [], {}
-        waiting = list(range(n_req))
-        t0 = time.perf_counter()
-        done = 0
-        while done < n_req:
-            now = time.perf_counter() - t0
-            still = []
-            for k in waiting:
-                i = k if pool is None else pool[k % len(pool)]
-                it = its[i]
-                deps = [it.get("past_from"), it.get("future_from")]
-                if (arrivals is not None and arrivals[k] > now) or any(d is not None and d not in res for d in deps):
-                    still.append(k)
-                    continue
-                if deps[0] is not None or deps[1] is not None:
-                    it = dict(it)
-                    for name, d in zip(("past", "future"), deps):
-                        if d is not None:
-                            it[name] = res[d]["recon"]
-                            it.pop(name + "_from")
-                tickets[srv.submit(it)] = i
-            waiting = still
-            if srv.poll():
-                for t in srv.finished():
-                    r = srv.result(t)
-                    lat.append(r["latency_ms"])
-                    res[tickets.pop(t)] = r
-                    done += 1
-            else:
-                time.sleep(0.0002)
-        return time.perf_counter() - t0, lat, res
+        return serve(srv, its, pool, arrivals)
 
     serve_all()  # warm
     barrier()

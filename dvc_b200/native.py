@@ -193,13 +193,15 @@ class Context:
                                           C.c_ubyte(int(crc)), C.c_float(rate_lower_bound)))
         return dec, rate.value, lr
 
-    def _frame_array(self, items):
+    def _frame_array(self, items, copy_recon=True):
         """ctypes frame array.  An item may name another item's decoded output as
         a reference with past_from / future_from (its index); the pointer then
-        equals that item's recon pointer, which dvc_session_create resolves."""
+        equals that item's recon pointer, which dvc_session_create resolves.
+        copy_recon=False passes the caller's starting content itself, for calls
+        that only read it (dvc_server_submit copies its inputs)."""
         keep, arr, outs = [], (WZFrame * len(items))(), []
         recs = [np.zeros((it["height"], it["width"]), np.uint8) if it.get("recon") is None else
-                np.ascontiguousarray(it["recon"], np.uint8).copy() for it in items]
+                np.array(it["recon"], np.uint8, copy=True if copy_recon else None, order="C") for it in items]
         for i, it in enumerate(items):
             w, h = it["width"], it["height"]
             past = recs[it["past_from"]] if it.get("past_from") is not None else \
@@ -339,7 +341,7 @@ class Server:
         self._meta = {}
 
     def submit(self, item):
-        arr, keep, qbits = self.ctx._frame_array([item])
+        arr, keep, qbits = self.ctx._frame_array([item], copy_recon=False)
         t = C.c_longlong(0)
         self.ctx.check(lib().dvc_server_submit(self._h, arr, C.byref(t)))
         self._meta[t.value] = (item["width"], item["height"], qbits[0])
