@@ -419,6 +419,12 @@ def main():
         per_unit = json.load(open(tpath)).get("dram_bytes_per_block_iteration")
         if per_unit is not None:
             traffic = per_unit * units_per_launch
+    # compulsory device I/O of the whole decode, per CIF WZ frame: the past and
+    # future frames, their two 4x-size half-pel planes, the decoded frame, each
+    # bitplane's accumulated syndrome (N/8 bytes, N = 6336) and CRC byte, and the
+    # 8x8 block-mode map; over the batched step time, against the same peak
+    frame_io = len(its) * (11 * fs + fs // 64) + qb * (6336 // 8 + 1)
+    frame_io_gbs = frame_io / (step_ms / 1e3) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -460,6 +466,12 @@ def main():
                                          "reads)" % alg_bytes_unit,
                          "units_per_launch": units_per_launch,
                          "aggregate_achieved": aggregate, "aggregate_frac": aggregate / peak,
+                         "frame_io": {"bytes_per_frame": frame_io / len(its), "achieved": frame_io_gbs,
+                                      "frac": frame_io_gbs / peak,
+                                      "note": "compulsory I/O of the whole WZ-frame decode (references, half-pel "
+                                              "planes, output, syndromes and CRCs, mode map) at the batched rate: "
+                                              "the path is bound by its gathers and compute, not by moving "
+                                              "these bytes"},
                          "note": "4-byte phi values gathered at random from a packed 170 MB table whose hot part "
                                  "stays in L2 (92% L2 hits, ~70 KB of DRAM traffic per block-iteration in ncu); the "
                                  "kernel is bound by the latency of those L2 gathers and by L1TEX throughput, not by "

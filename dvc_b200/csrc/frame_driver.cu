@@ -368,7 +368,11 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     // every lockstep bitplane step, for 7% more BP work at 8 blocks than at 1
     // on 640 CIF frames, where 8 blocks decode 2x faster than 1 and 3% faster
     // than 4 or 12); at least 8 blocks per codeword, more when SMs are idle
-    int k = std::max(8, sms / std::max(1, std::max(nf, concurrent)));
+    // DVC_LDPCA_SPEC_FLOOR replaces the floor of 8 (the autotuner's setting),
+    // DVC_LDPCA_SPEC fixes the width outright
+    int floor_k = 8;
+    if (const char *e = getenv("DVC_LDPCA_SPEC_FLOOR")) floor_k = std::max(1, std::min(32, atoi(e)));
+    int k = std::max(floor_k, sms / std::max(1, std::max(nf, concurrent)));
     if (const char *e = getenv("DVC_LDPCA_SPEC")) k = atoi(e);
     spec_k_ = std::max(1, std::min(32, k));
     if (!spec_.ensure(ldpca_spec_scratch_bytes(n, nf, spec_k_), alloc_stream_))

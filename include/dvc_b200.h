@@ -33,7 +33,14 @@ typedef struct dvc_ctx dvc_ctx;
  * the GF(2) inverses (built on first use when absent).
  * Replaces InitCUDA + LDPCA_CUDA_Init_Variable + *_Init_Buffer
  * (LDPCA_cuda.h:16-17, noiseModel_kernel.h:13, updateSI_kernel.h:13,
- * forwardME_kernel.h:11, motionLearning_kernel.h:11; called at main.cpp:92-103). */
+ * forwardME_kernel.h:11, motionLearning_kernel.h:11; called at main.cpp:92-103).
+ * Launch shape of the LDPCA ladder kernel, from the environment (the values
+ * dvc_b200.autotune chooses by measurement; decoded output never depends on
+ * them): DVC_LDPCA_THREADS = 512 or 1024 threads per codeword block (default
+ * 1024), read here; DVC_LDPCA_SPEC_FLOOR = 1..32, the least number of
+ * speculative blocks per codeword in a frame batch (default 8), and
+ * DVC_LDPCA_SPEC = 1..32, a fixed number instead, both read when a batch is
+ * prepared. */
 int dvc_create(const char *data_dir, const char *table_dir, int device, dvc_ctx **out);
 
 /* Release everything the context owns.  Replaces LDPCA_CUDA_Free_Variable and
