@@ -60,7 +60,9 @@ bool Context::init(const char *data, const char *tables, int dev) {
   mkdir(table_dir.c_str(), 0755);
   if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return false;
   if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
-  if (const char *nt = getenv("DVC_LDPCA_THREADS")) set_ldpca_threads(atoi(nt));
+  // process-wide, set by every context creation (1024 unless the variable asks for 512)
+  const char *nt = getenv("DVC_LDPCA_THREADS");
+  set_ldpca_threads(nt ? atoi(nt) : 1024);
 
   // library-exact math tables: load, or sweep the C library once and cache
   const std::string xpath = table_dir + "/xlm_tables.bin";

@@ -1,0 +1,37 @@
+"""The autotuner's measurement on the device: a small batched CIF session decoded
+under three launch shapes of the LDPCA ladder (threads per codeword block and
+speculative-width floor), each a fresh context; tune() requires every shape
+to decode the same frames, rates and ladder codes."""
+import os
+
+import numpy as np
+import pytest
+
+from dvc_b200 import autotune as at
+
+pytestmark = pytest.mark.gpu
+
+
+def test_launch_shapes_decode_identically():
+    from dvc_b200 import native
+    items = at.workload(n_streams=2, n_frames=9)
+    settings = [{at.ENV_THREADS: "1024", at.ENV_FLOOR: "8"}, {at.ENV_THREADS: "512", at.ENV_FLOOR: "1"},
+                {at.ENV_THREADS: "1024", at.ENV_FLOOR: "32"}]
+
+    def measure(setting):
+        ctx = native.Context(0)
+        try:
+            ses = ctx.session(items, max_batch=4, streams=2)
+            try:
+                ms = [ses.run() for _ in range(3)]  # direct, captured, replayed
+                return ms, [ses.frame(i) for i in range(len(items))]
+            finally:
+                ses.close()
+        finally:
+            ctx.close()
+
+    before = {k: os.environ.get(k) for k in (at.ENV_THREADS, at.ENV_FLOOR)}
+    best, results = at.tune(measure, settings)
+    assert len(results) == 3 and best["setting"] in settings
+    assert all(np.isfinite(r["ms"]).all() and min(r["ms"]) > 0 for r in results)
+    assert {k: os.environ.get(k) for k in (at.ENV_THREADS, at.ENV_FLOOR)} == before
