@@ -1,7 +1,8 @@
-"""The bench's serving loop (bench.serve) against a fake server on the CPU:
-every request is served once, a frame that names another frame's output as its
-reference is submitted only after that output exists and receives it, and the
-loop ends whichever polls finish the work."""
+"""The bench's host side on the CPU.  Its serving loop (bench.serve) against a
+fake server: every request is served once, a frame that names another frame's
+output as its reference is submitted only after that output exists and
+receives it, and the loop ends whichever polls finish the work.  Its intra step
+(bench.intra_starts): the frames' starting content."""
 import os
 import sys
 
@@ -118,3 +119,24 @@ def test_serve_pool_with_arrivals():
     dt, lat, res = bench.serve(srv, its, pool, arrivals, poll_every=3)
     assert len(lat) == 40 and len(srv.submitted) == 40
     assert dt >= arrivals[-1]
+
+
+def test_intra_starts_match_a_direct_decode():
+    """bench.intra_starts: every frame's starting content equals the key-frame
+    content with that frame's intra blocks decoded over it (frames without
+    intra blocks: the key-frame content itself)."""
+    from dvc_b200 import bitstream as bs, encoder, intra, synth
+    ori, key = synth.make_sequence("cif", 9, 77)
+    streams, ib = {}, {}
+    for gq in ((4, 3), (4, 8)):
+        wz, b = encoder.encode_sequence_intra(ori, gq[0], gq[1], 30, 1, 1, 1)
+        streams[gq], ib[gq] = bs.parse_wz(wz), b
+    starts = bench.intra_starts(streams, ib, key)
+    for gq, st in streams.items():
+        want = np.array(key, copy=True)
+        for m, (px, _) in intra.decode_all(st, ib[gq], key).items():
+            want[m] = px
+        for m in range(key.shape[0]):
+            got = starts[gq][m]
+            assert got.dtype == np.uint8 and got.flags.c_contiguous and np.array_equal(got, want[m]), (gq, m)
+    assert any(fr.intra_mode for fr in streams[(4, 8)].frames.values())
