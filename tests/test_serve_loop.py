@@ -140,3 +140,31 @@ def test_intra_starts_match_a_direct_decode():
             got = starts[gq][m]
             assert got.dtype == np.uint8 and got.flags.c_contiguous and np.array_equal(got, want[m]), (gq, m)
     assert any(fr.intra_mode for fr in streams[(4, 8)].frames.values())
+
+
+def test_serving_overlapped_with_the_intra_step():
+    """The e2e step's form: intra blocks decoded on a pool while the loop
+    submits each frame once its stream's starting content is ready
+    (start_of); the results equal those of decoding the intra blocks first."""
+    from concurrent.futures import ThreadPoolExecutor
+    from dvc_b200 import bitstream as bs, encoder, synth
+    ori, key = synth.make_sequence("cif", 9, 78)
+    streams, ib = {}, {}
+    for gq in ((2, 1), (4, 5), (4, 8)):
+        wz, b = encoder.encode_sequence_intra(ori, gq[0], gq[1], 30, 1, 1, 1)
+        streams[gq], ib[gq] = bs.parse_wz(wz), b
+    its, lev, src = bench.items(streams, key, bench.intra_starts(streams, ib, key))
+    want = bench.serve(FakeServer(per_poll=3, idle=4), its)[2]
+    for it in its:  # the step must bring its own starting content
+        it["recon"] = np.zeros_like(it["recon"])
+    with ThreadPoolExecutor(2) as ex:
+        fut = bench.intra_starts_async(ex, streams, ib, key)
+
+        def start_of(i):
+            gq, m = src[i]
+            return fut[gq].result()[m] if fut[gq].done() else None
+
+        got = bench.serve(FakeServer(per_poll=3, idle=4), its, start_of=start_of)[2]
+    assert sorted(got) == sorted(want) == list(range(len(its)))
+    for i in want:
+        assert np.array_equal(got[i]["recon"], want[i]["recon"]), i
