@@ -145,3 +145,22 @@ def test_oracle_intra_reads_encoder_blocks(qp, content):
     assert not out[~px].any()  # pixels of other blocks are left alone
     with pytest.raises(RuntimeError):  # a string cut short inside the last block
         po.intra_decode_frame(geom, fr, data[:max(1, (end - 40) // 8)], 5, np.zeros((h, w), np.uint8))
+
+
+def test_oracle_cif_intra_deblocked_frame_matches_reference(golden_dir):
+    """CIF geometry through the oracle's intra, WZ and deblocking paths: the
+    first decoded frame of a CIF GOP-4 sequence with SkipBlock, IntraMode and
+    DeblockingFilter on (302 intra 8x8 blocks), against the reference decoder."""
+    g = load(golden_dir, "seq_cif_g4_q6_full.npz")
+    ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
+    st = bs.parse_wz(g["wz"].tobytes())
+    m = bs.sequence_order(st.n_frames, st.gop)[0][0]
+    assert (st.frames[m].mode == 1).sum() > 0 and st.deblock
+    res = po.decode_sequence(st, key, ori, {}, {}, frames={m}, intra_bitstream=g["intra"].tobytes())
+    assert np.array_equal(res["recon"][m], g["dec_y"][m])
+    k = list(g["frames"]).index(m)
+    assert res["bits"][m] == g["bits"][k]
+    assert "%.2f" % res["psnr"][m] == "%.2f" % g["psnr"][k]
+    qb = len(res["planes"][m][0])
+    assert np.array_equal(res["planes"][m][0], g["ld_start"][:qb])
+    assert np.array_equal(res["planes"][m][1], g["ld_accepted"][:qb])
