@@ -115,18 +115,20 @@ class _Geom:
         self.__dict__.update(kw)
 
 
+@pytest.mark.parametrize("size", [(144, 176), (288, 352)])
 @pytest.mark.parametrize("qp", [0, 12, 30, 51])
 @pytest.mark.parametrize("content", ["noise", "ramp", "half_intra"])
-def test_oracle_intra_reads_encoder_blocks(qp, content):
+def test_oracle_intra_reads_encoder_blocks(qp, content, size):
     """The oracle's CAVLC reader on intra blocks written by the library's
     encoder (dvc_intra_encode_frame): every bit consumed and every intra pixel
-    equal to the reconstruction the encoder reports.  IntraQP 0 on noise takes
+    equal to the reconstruction the encoder reports, and the library's host
+    decoder (dvc_intra_decode_frame) equal to the oracle.  IntraQP 0 on noise takes
     the level_prefix 15 escape (about 4,500 times in the frame) and the 6-bit
     coeff_token of nC >= 8 (about 1,600 blocks); IntraQP 51 leaves mostly empty
     blocks."""
     from dvc_b200 import intra
-    rng = np.random.default_rng(qp * 7 + len(content))
-    h, w = 144, 176
+    rng = np.random.default_rng(qp * 7 + len(content) + size[0])
+    h, w = size
     if content == "noise":
         ori = rng.integers(0, 256, (h, w), dtype=np.uint8)
     else:
@@ -143,6 +145,15 @@ def test_oracle_intra_reads_encoder_blocks(qp, content):
     px = np.kron(mode, np.ones((8, 8), np.uint8)).astype(bool)
     assert np.array_equal(out[px], rec[px])
     assert not out[~px].any()  # pixels of other blocks are left alone
+    # the library's own host decoder reads the same string to the same pixels and end
+    import ctypes as C
+    from dvc_b200 import native
+    lib_out = np.zeros((h, w), np.uint8)
+    off = C.c_size_t(5)
+    assert native.lib().dvc_intra_decode_frame(data.ctypes.data_as(C.c_void_p), data.size, C.byref(off), w, h, qp,
+                                               fr.mode.ctypes.data_as(C.c_void_p),
+                                               lib_out.ctypes.data_as(C.c_void_p)) == native.DVC_OK
+    assert off.value == end and np.array_equal(lib_out, out)
     with pytest.raises(RuntimeError):  # a string cut short inside the last block
         po.intra_decode_frame(geom, fr, data[:max(1, (end - 40) // 8)], 5, np.zeros((h, w), np.uint8))
 
