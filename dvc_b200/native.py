@@ -110,6 +110,12 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def _addr(a):
+    """The address of an array's data for a pointer field of a ctypes struct
+    (the caller keeps the array alive as long as the struct is used)."""
+    return None if a is None else a.ctypes.data
+
+
 class Context:
     """A decoder context on one CUDA device (dvc_create / dvc_destroy)."""
 
@@ -215,10 +221,10 @@ class Context:
             rec = recs[i]
             pmode = None if it.get("past_mode") is None else np.ascontiguousarray(it["past_mode"], np.uint8)
             keep += [past, fut, mode, acr, crc, acc, rec, pmode]
-            arr[i] = WZFrame(w, h, it["qindex"], it["past_idx"], it["future_idx"], it["cur_idx"], _ptr(past),
-                             _ptr(fut), _ptr(mode), it.get("skip_mode", 0), it.get("intra_mode", 0), _ptr(acr),
-                             _ptr(crc), _ptr(acc), _ptr(rec), 0, None, None, None,
-                             it.get("deblock", 0), it.get("intra_qp", 0), _ptr(pmode))
+            arr[i] = WZFrame(w, h, it["qindex"], it["past_idx"], it["future_idx"], it["cur_idx"], _addr(past),
+                             _addr(fut), _addr(mode), it.get("skip_mode", 0), it.get("intra_mode", 0), _addr(acr),
+                             _addr(crc), _addr(acc), _addr(rec), 0, None, None, None,
+                             it.get("deblock", 0), it.get("intra_qp", 0), _addr(pmode))
             outs.append(len(crc))
         return arr, keep, outs
 
