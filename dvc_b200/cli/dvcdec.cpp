@@ -253,7 +253,7 @@ WzStream read_wz(const std::string &path) {
         // the JBIG-coded 8x8 mode map that follows a set flag (wzbitstream.cpp:38-66)
         std::vector<uint8_t> map(nb88);
         size_t used = 0;
-        if (dvc_jbig_decode_mode_map(&d[pos], d.size() - pos, s.w / 8, s.h / 8, map.data(), &used) != DVC_OK)
+        if (dvc_jbig_decode_mode_map(d.data() + pos, d.size() - pos, s.w / 8, s.h / 8, map.data(), &used) != DVC_OK)
           die("JBIG mode map of frame " + std::to_string(fr.idx) + " could not be decoded");
         pos += used;
         (k == 0 ? fr.skip_bits : fr.intra_bits) = (int)(used << 3) + 1;

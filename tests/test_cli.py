@@ -57,6 +57,25 @@ def test_cli_rejects_bad_arguments(tmp_path):
     assert r.returncode != 0 and "Too few parameters" in r.stderr
 
 
+def test_cli_refuses_damaged_wz_bitstreams(tmp_path, golden_dir):
+    """Truncated WZ bitstreams (cut in headers, AC ranges, JBIG mode maps and
+    syndromes) and bad header fields end with an error message and a non-zero
+    exit, never a signal; the bitstream is parsed before any GPU work."""
+    g = dict(np.load(os.path.join(golden_dir, "seq_qcif_still_g4_q4_full.npz")))
+    d, cfg = _setup(tmp_path, g)
+    wz = g["wz"].tobytes()
+    path = os.path.join(d, "seq.wz")
+    cases = [wz[:n] for n in sorted(set(list(range(0, 40)) + list(range(40, len(wz) - 1, max(1, len(wz) // 40)))))]
+    cases += [bytes([7]) + wz[1:], wz[:1] + bytes([0]) + wz[2:], wz[:1] + bytes([9]) + wz[2:], wz[:3] + bytes([0]) + wz[4:]]
+    for data in cases:
+        with open(path, "wb") as f:
+            f.write(data)
+        r = subprocess.run([_cli(), "-d", cfg], capture_output=True, text=True, timeout=60)
+        assert r.returncode > 0, (len(data), r.returncode, r.stderr[-300:])
+        assert any(m in r.stderr for m in ("truncated", "shorter than its header", "could not be decoded",
+                                           "Unsupport resolution", "Qindex out of range", "GOP must be")), r.stderr
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("seq", ["qcif_g4_q8", "cif_g2_q2", "qcif_still_g2_q4_skip", "cif_g4_q6_intra",
                                  "cif_g4_q6_full", "qcif_g2_q8_own_full"])
