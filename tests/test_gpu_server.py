@@ -56,3 +56,40 @@ def test_server_refuses_frame_above_budget(gpu_ctx):
         srv.submit(it)
     assert ex.value.code == native.DVC_E_NOMEM
     srv.close()
+
+
+def test_bench_e2e_form_matches_session(gpu_ctx):
+    """The bench's end-to-end form on a small workload: intra blocks decoded on
+    a host pool while the server decodes the frames whose starting content is
+    ready (bench.serve with start_of), second-level frames submitted with their
+    references' results; every frame equals the device-resident session's."""
+    import sys
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    ori, key = synth.make_sequence("cif", 9, 91)
+    streams, ib = {}, {}
+    for gq in ((2, 2), (4, 5), (4, 8)):
+        wz, b = encoder.encode_sequence_intra(ori, gq[0], gq[1], 30, 1, 1, 1)
+        streams[gq], ib[gq] = bs.parse_wz(wz), b
+    its, lev, src = bench.items(streams, key, bench.intra_starts(streams, ib, key))
+    assert max(lev) == 1
+    ses = gpu_ctx.session(its, max_batch=4, streams=2)
+    srv = gpu_ctx.server(mem_budget_bytes=4 << 30, streams=2, max_cohort=4)
+    try:
+        ses.run()
+        with ThreadPoolExecutor(2) as ex:
+            fut = bench.intra_starts_async(ex, streams, ib, key)
+
+            def start_of(i):
+                gq, m = src[i]
+                return fut[gq].result()[m] if fut[gq].done() else None
+
+            _, lat, served = bench.serve(srv, its, start_of=start_of, poll_every=2)
+        assert sorted(served) == list(range(len(its))) and len(lat) == len(its)
+        for i in range(len(its)):
+            rec, bits, _ = ses.frame(i)
+            assert np.array_equal(served[i]["recon"], rec) and served[i]["wz_bits"] == bits, i
+    finally:
+        srv.close()
+        ses.close()
