@@ -31,8 +31,13 @@ Our arm prints one JSON line with:
   plain   the one-frame-at-a-time drop-in (one dvc_decode_wz_frames call per
           frame) with per-frame latency p50/p99;
   roofline, cpu_baseline, clocks, gpu_launches.
---impl reference times the reference decoder's own CPU path (oracle/_ref/DvcDec,
-ParallelMode 1 with every host core) on a bounded sample of the same workload.
+--impl reference times the reference codec's own CPU path on the same
+sequences and settings: streams encoded by the reference encoder
+(oracle/_ref/DvcEnc), whole GOPs decoded by the reference decoder
+(oracle/_ref/DvcDec, ParallelMode 1 with every host core), a fixed stratified
+sample over every (GOP, QIndex) stream and both levels, the workload's rate
+estimated from the per-stream times; plus ParallelMode 0 on one core for one
+frame.  That process loads none of this repository's native libraries.
 Under torchrun each rank decodes its own replica (weak scaling, no collective
 on the data path); rank 0 prints the max-over-ranks result.
 """
@@ -236,30 +241,85 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def ref_cpu_sample(ori, key, streams, q, cores, workdir):
-    """Decode one WZ frame (the first GOP) of the Q stream with the reference CPU decoder."""
-    from oracle import refrun
-    from dvc_b200 import synth, bitstream as bs
-    import struct
-    d = tempfile.mkdtemp(dir=workdir)
-    oy, ky, sf = os.path.join(d, "o.yuv"), os.path.join(d, "k.yuv"), os.path.join(d, "s.txt")
-    synth.write_yuv420(oy, ori[:3])
-    synth.write_yuv420(ky, key[:3])
-    synth.write_frame_stat(sf, 3)
-    from dvc_b200 import encoder
-    wzb, ib = encoder.encode_sequence_intra(ori[:3], 2, q, INTRA_QP, 1, 1, 1)
-    wz = os.path.join(d, "s.wz")
-    open(wz, "wb").write(wzb)
-    intra = os.path.join(d, "s.intra")
-    open(intra, "wb").write(ib)
-    t0 = time.time()
-    r = refrun.decode(oy, wz, intra, ky, sf, mode=1 if cores > 1 else 0, cores=cores)
-    wall = time.time() - t0
-    dec_t = None
-    for line in r["rd"].splitlines():
-        if line.startswith("Total decoding time:"):
-            dec_t = float(line.split(":")[1].split()[0])
-    return dec_t if dec_t else wall
+class RefStreams:
+    """The bench workload for the reference's own CPU codec: the same synthetic
+    sequence (dvc_b200.synth, numpy only) written to YUV files and every
+    (GOP, QIndex) stream encoded by the reference encoder (oracle/_ref/DvcEnc,
+    SkipBlock 1, IntraMode 1, DeblockingFilter 1, IntraQP 30), so that the
+    process timing the reference loads none of this repository's native code.
+    Samples are whole GOPs decoded by the reference decoder (oracle/_ref/DvcDec)
+    with its -startFrame/-endFrame range; the time is the decoder's own
+    "Total decoding time" (its timed region, DvcDec/src/main.cpp:109-145)."""
+
+    def __init__(self, workdir):
+        from oracle import refrun
+        from dvc_b200 import synth
+        self.refrun = refrun
+        ori, key = synth.make_sequence(KIND, N_FRAMES, SEED)
+        self.dir = workdir
+        self.oy, self.ky = os.path.join(workdir, "ori.yuv"), os.path.join(workdir, "key.yuv")
+        self.stat = os.path.join(workdir, "stat.txt")
+        synth.write_yuv420(self.oy, ori)
+        synth.write_yuv420(self.ky, key)
+        synth.write_frame_stat(self.stat, N_FRAMES)
+        self.streams = {}
+        for g in GOPS:
+            for q in QS:
+                d = refrun._workdir(workdir)  # holds the ladder directory the encoder opens
+                wz, ib, _ = refrun.encode(self.oy, self.ky, N_FRAMES, "CIF", g, q, skip=1, intra=1,
+                                          intra_qp=INTRA_QP, deblock=1, workdir=d)
+                self.streams[(g, q)] = (wz, ib)
+
+    @staticmethod
+    def wz_frames(g):
+        """WZ frames of a (g) stream in the bench workload."""
+        return sum(e - b - 1 for b, e in ((i, min(i + g, N_FRAMES - 1)) for i in range(0, N_FRAMES - 1, g)))
+
+    def decode_gop(self, gq, k, mode, cores):
+        """Decode GOP k of stream gq; returns (decoder seconds, WZ frames decoded)."""
+        g = gq[0]
+        wz, ib = self.streams[gq]
+        r = self.refrun.decode(self.oy, wz, ib, self.ky, self.stat, mode=mode, cores=cores, start=k * g,
+                               end=(k + 1) * g)
+        t = None
+        for line in r["rd"].splitlines():
+            if line.startswith("Total decoding time:"):
+                t = float(line.split(":")[1].split()[0])
+        return (t if t else r["seconds"]), g - 1
+
+
+def ref_plan(n_samples, per_step=4):
+    """A fixed stratified sample of the workload: step i decodes one GOP of each
+    of `per_step` streams, cycling through all (GOP, QIndex) streams; the GOP
+    index moves along each stream's sequence from one visit to the next, so a
+    run covers every stream, both levels of GOP 4 and several parts of the
+    sequences."""
+    keys = [(g, q) for g in GOPS for q in QS]
+    plan = []
+    for i in range(n_samples):
+        step = []
+        for j in range(per_step):
+            c = i * per_step + j
+            gq = keys[c % len(keys)]
+            visit = c // len(keys)
+            n_gops = (N_FRAMES - 1) // gq[0]
+            step.append((gq, (7 * visit + 3 * QS.index(gq[1])) % n_gops))
+        plan.append(step)
+    return plan
+
+
+def ref_estimate(samples):
+    """WZ frames/s of the whole workload from per-stream samples: every stream's
+    seconds per WZ frame, weighted by its share of the workload's frames
+    (streams not sampled are left out of both sides)."""
+    per = {}
+    for gq, t, n in samples:
+        a = per.setdefault(gq, [0.0, 0])
+        a[0] += t
+        a[1] += n
+    frames = sum(RefStreams.wz_frames(gq[0]) for gq in per)
+    secs = sum(RefStreams.wz_frames(gq[0]) * t / n for gq, (t, n) in per.items())
+    return frames / secs, frames
 
 
 def run_reference(args, rank):
@@ -269,23 +329,40 @@ def run_reference(args, rank):
     if not refrun.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
         return
-    ori, key, streams, _ = workload()
     cores = os.cpu_count() or 1
-    tmp = tempfile.mkdtemp()
-    for i in range(args.warmup):
-        ref_cpu_sample(ori, key, streams, QS[i % len(QS)], cores, tmp)
-    times = []
-    for i in range(args.steps):
-        times.append(ref_cpu_sample(ori, key, streams, QS[i % len(QS)], cores, tmp))
-    fps = len(times) / sum(times)
+    rs = RefStreams(tempfile.mkdtemp())
+    plan = ref_plan(args.warmup + args.steps)
+    for step in plan[:args.warmup]:
+        for gq, k in step:
+            rs.decode_gop(gq, k, 1, cores)
+    samples, step_s = [], []
+    for step in plan[args.warmup:]:
+        tot = 0.0
+        for gq, k in step:
+            t, n = rs.decode_gop(gq, k, 1, cores)
+            samples.append((gq, t, n))
+            tot += t
+        step_s.append(tot)
+    fps, covered = ref_estimate(samples)
+    # ParallelMode 0 (the sequential decoder, one core) on one GOP-2 frame at QIndex 4
+    t0, n0 = rs.decode_gop((2, 4), 0, 0, 1)
+    total_frames = sum(RefStreams.wz_frames(g) for g in GOPS for _ in QS)
     line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": "WZ frames/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(step_s)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
-            "config": {"workload": "CIF 352x288 GOP2, one WZ frame per step, QIndex cycling 1..8, SkipBlock 1, "
-                                   "IntraMode 1, DeblockingFilter 1, reference DvcDec ParallelMode 1 on every host core",
-                       "frames_per_step": 1},
+            "config": {"workload": "CIF 352x288, 65-frame sequences at GOP 2 and GOP 4, QIndex 1..8 -> %d WZ frames "
+                                   "(SkipBlock 1, IntraMode 1, DeblockingFilter 1, IntraQP 30), encoded by the "
+                                   "reference encoder; reference DvcDec ParallelMode 1 on every host core"
+                                   % total_frames,
+                       "frames_per_step": float(np.mean([sum(g - 1 for (g, _), _ in st) for st in plan[args.warmup:]])),
+                       "estimate": "stratified: seconds per WZ frame of each (GOP, QIndex) stream from its "
+                                   "sampled GOPs, weighted by the stream's frames in the workload",
+                       "frames_covered": covered, "samples": len(samples)},
             "cpu_baseline": {"value": fps, "unit": "WZ frames/s", "cores": cores, "kind": "reference",
-                             "sample": "1 CIF WZ frame per step (3-frame GOP-2 sequence), Q cycling 1..8"},
+                             "sample": "%d GOPs over the %d streams (4 per step), reference DvcDec ParallelMode 1, "
+                                       "decoder-reported decoding time" % (len(samples), len(GOPS) * len(QS))},
+            "mode0": {"value": n0 / t0, "unit": "WZ frames/s", "cores": 1,
+                      "sample": "reference DvcDec ParallelMode 0 (sequential), the first GOP-2 WZ frame at QIndex 4"},
             "e2e": {"value": fps, "unit": "WZ frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -460,10 +537,13 @@ def main():
             from oracle import refrun
             if refrun.ref_available():
                 cores = os.cpu_count() or 1
-                t = ref_cpu_sample(ori, key, streams, 4, cores, tempfile.mkdtemp())
-                cpu = {"value": 1.0 / t, "unit": "WZ frames/s", "cores": cores, "kind": "reference",
-                       "sample": "1 CIF WZ frame, Q4, reference DvcDec ParallelMode 1 with every core "
-                                 "(decoder-reported decoding time)"}
+                rs = RefStreams(tempfile.mkdtemp())
+                samples = [(gq, *rs.decode_gop(gq, k, 1, cores)) for gq, k in ref_plan(4)[0] + ref_plan(4)[2]]
+                fps, _ = ref_estimate(samples)
+                cpu = {"value": fps, "unit": "WZ frames/s", "cores": cores, "kind": "reference",
+                       "sample": "8 GOPs of 8 streams (GOP 2 and 4, QIndex 1-4 and 5-8 in turn) of the same sequence, "
+                                 "encoded by the reference encoder, reference DvcDec ParallelMode 1 with every core "
+                                 "(decoder-reported decoding time), weighted by the streams' frames"}
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "WZ frames/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": "failed: %s" % str(ex)[:200]}

@@ -132,6 +132,116 @@ extern "C" int dvc_ldpca_decode(dvc_ctx *ctx, int n, int count, const float *lr,
   return ldpca_run(ctx->c, n, count, lr, acc, crc, decoded, results, entropy, max_iter, nullptr, nullptr);
 }
 
+extern "C" int dvc_ldpca_decode_batch(dvc_ctx *ctx, int count, const int *n, const float *lr, const uint8_t *acc,
+                                      const uint8_t *crc, const int *start, uint8_t *decoded, int *results,
+                                      float *entropy, int max_iter, long long *bp_iterations, double *kernel_ms) {
+  if (!ctx) return DVC_E_ARG;
+  Context &c = ctx->c;
+  if (count <= 0 || count > (1 << 22) || !n || !lr || !acc || !crc || !results || max_iter <= 0) {
+    c.err = "dvc_ldpca_decode_batch: bad arguments";
+    return DVC_E_ARG;
+  }
+  const dvc::LadderDev *Lc = c.ladder(6336), *Lq = c.ladder(1584);
+  if (!Lc || !Lq) {
+    c.err = "dvc_ldpca_decode_batch: ladders missing";
+    return DVC_E_DATA;
+  }
+  std::vector<dvc::LdpcaBatchCw> cw(count);
+  std::vector<int> lists;
+  lists.reserve(count);
+  long long lr_off = 0, byte_off = 0;
+  for (int i = 0; i < count; i++) {
+    if (n[i] != 1584 && n[i] != 6336) {
+      c.err = "dvc_ldpca_decode_batch: codeword " + std::to_string(i) + " has length " + std::to_string(n[i]) +
+              " (1584 or 6336)";
+      return DVC_E_ARG;
+    }
+    cw[i].cif = n[i] == 6336;
+    cw[i].crc = crc[i];
+    cw[i].given_start = start ? start[i] : -1;
+    if (start && (start[i] < 0 || start[i] > 64)) {
+      c.err = "dvc_ldpca_decode_batch: start level out of range";
+      return DVC_E_ARG;
+    }
+    cw[i].lr_off = lr_off;
+    cw[i].acc_off = byte_off / 8;
+    cw[i].dec_off = byte_off;
+    lr_off += n[i];
+    byte_off += n[i];
+  }
+  for (int i = 0; i < count; i++)
+    if (cw[i].cif) lists.push_back(i);
+  const int n_cif = (int)lists.size();
+  for (int i = 0; i < count; i++)
+    if (!cw[i].cif) lists.push_back(i);
+  if (!c.bt_lr.ensure((size_t)lr_off * 4) || !c.bt_acc.ensure((size_t)byte_off / 8) ||
+      !c.bt_dec.ensure((size_t)byte_off) || !c.bt_res.ensure((size_t)count * 16) || !c.bt_ent.ensure((size_t)count * 4) ||
+      !c.bt_cw.ensure(sizeof(dvc::LdpcaBatchCw) * count + sizeof(int) * count + 64) ||
+      !c.bt_state.ensure(dvc::ldpca_batch_state_bytes(count))) {
+    c.err = "device allocation failed";
+    return DVC_E_NOMEM;
+  }
+  dvc::LdpcaBatch A{};
+  A.L_cif = *Lc;
+  A.L_qcif = *Lq;
+  A.xt = c.xlm;
+  uint8_t *cwb = c.bt_cw.as<uint8_t>();
+  A.cw = (const dvc::LdpcaBatchCw *)cwb;
+  int *list_dev = (int *)(cwb + sizeof(dvc::LdpcaBatchCw) * count);
+  A.cif = list_dev;
+  A.qcif = list_dev + n_cif;
+  A.n_cif = n_cif;
+  A.n_qcif = count - n_cif;
+  A.last_cif = Lc->num_codes - 1;
+  A.last_qcif = Lq->num_codes - 1;
+  A.ctr = (int *)(list_dev + count);
+  A.work = (unsigned long long *)(A.ctr + 2);
+  A.state = c.bt_state.as<dvc::LdpcaBatchState>();
+  A.slot_bits = (uint32_t *)(c.bt_state.as<uint8_t>() + sizeof(dvc::LdpcaBatchState) * count);
+  A.lr = c.bt_lr.as<float>();
+  A.acc = c.bt_acc.as<uint8_t>();
+  A.decoded = decoded ? c.bt_dec.as<uint8_t>() : nullptr;
+  A.results = c.bt_res.as<int>();
+  A.entropy = c.bt_ent.as<float>();
+  A.max_iter = max_iter;
+  cudaStream_t s = c.stream;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  int st;
+  if ((st = cuda_status(c, cudaMemcpyAsync(c.bt_lr.p, lr, (size_t)lr_off * 4, cudaMemcpyHostToDevice, s), "H2D lr")) ||
+      (st = cuda_status(c, cudaMemcpyAsync(c.bt_acc.p, acc, (size_t)byte_off / 8, cudaMemcpyHostToDevice, s), "H2D acc")) ||
+      (st = cuda_status(c, cudaMemcpyAsync(cwb, cw.data(), sizeof(dvc::LdpcaBatchCw) * count, cudaMemcpyHostToDevice, s),
+                        "H2D codewords")) ||
+      (st = cuda_status(c, cudaMemcpyAsync(list_dev, lists.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s),
+                        "H2D lists")))
+    return st;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (kernel_ms && ((st = cuda_status(c, cudaEventCreate(&e0), "event")) ||
+                    (st = cuda_status(c, cudaEventCreate(&e1), "event"))))
+    return st;
+  if (e0) cudaEventRecord(e0, s);
+  st = cuda_status(c, dvc::launch_ldpca_batch(A, count, sms, s), "ldpca batch launch");
+  if (e1) cudaEventRecord(e1, s);
+  unsigned long long work = 0;
+  if (!st && decoded)
+    st = cuda_status(c, cudaMemcpyAsync(decoded, c.bt_dec.p, (size_t)byte_off, cudaMemcpyDeviceToHost, s), "D2H dec");
+  if (!st)
+    st = cuda_status(c, cudaMemcpyAsync(results, c.bt_res.p, (size_t)count * 16, cudaMemcpyDeviceToHost, s), "D2H res");
+  if (!st && entropy)
+    st = cuda_status(c, cudaMemcpyAsync(entropy, c.bt_ent.p, (size_t)count * 4, cudaMemcpyDeviceToHost, s), "D2H ent");
+  if (!st) st = cuda_status(c, cudaMemcpyAsync(&work, A.work, 8, cudaMemcpyDeviceToHost, s), "D2H work");
+  if (!st) st = cuda_status(c, cudaStreamSynchronize(s), "ldpca batch sync");
+  if (!st && kernel_ms) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    *kernel_ms = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (!st && bp_iterations) *bp_iterations = (long long)work;
+  return st;
+}
+
 extern "C" int dvc_ldpca_encode(dvc_ctx *ctx, int n, int count, const uint8_t *bits, uint8_t *acc, uint8_t *crc) {
   if (!ctx) return DVC_E_ARG;
   Context &c = ctx->c;
@@ -179,7 +289,7 @@ extern "C" int dvc_LdpcaDecoder(dvc_ctx *ctx, int n, float *LR_intrinsic, const 
 }
 
 static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t *dbg_si0, float *dbg_alpha,
-                         uint8_t *dbg_si1);
+                         uint8_t *dbg_si1, float *dbg_lr = nullptr);
 
 extern "C" int dvc_decode_wz_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames) {
   return decode_frames(ctx, count, frames, nullptr, nullptr, nullptr);
@@ -190,8 +300,23 @@ extern "C" int dvc_debug_wz_frame(dvc_ctx *ctx, dvc_wz_frame *frame, uint8_t *si
   return decode_frames(ctx, 1, frame, si_initial, alpha, si_final);
 }
 
+extern "C" int dvc_debug_wz_frame_lr(dvc_ctx *ctx, dvc_wz_frame *frame, float *lr_planes) {
+  if (!ctx || !frame || !lr_planes) return DVC_E_ARG;
+  return decode_frames(ctx, 1, frame, nullptr, nullptr, nullptr, lr_planes);
+}
+
+extern "C" int dvc_recon_near_ties(dvc_ctx *ctx, long long *count) {
+  if (!ctx || !count) return DVC_E_ARG;
+  dvc::Context &c = ctx->c;
+  unsigned long long v = 0;
+  int st;
+  if ((st = cuda_status(c, cudaMemcpy(&v, c.near_ties.p, 8, cudaMemcpyDeviceToHost), "near-tie counter"))) return st;
+  *count = (long long)v;
+  return DVC_OK;
+}
+
 static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t *dbg_si0, float *dbg_alpha,
-                         uint8_t *dbg_si1) {
+                         uint8_t *dbg_si1, float *dbg_lr) {
   if (!ctx) return DVC_E_ARG;
   Context &c = ctx->c;
   if (count <= 0 || !frames) {
@@ -280,14 +405,16 @@ static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t 
     S.deblock_flag = ctx->dbf[i].as<uint8_t>();
   }
   dvc::DevBuf &dbg = ctx->dbg;
-  if (dbg_si0 || dbg_alpha || dbg_si1) {
-    if (!dbg.ensure(fs * 6)) {
+  const size_t lr_bytes = dbg_lr ? (size_t)dvc::qbits_per_block(frames[0].qindex) * (fs / 16) * 4 : 0;
+  if (dbg_si0 || dbg_alpha || dbg_si1 || dbg_lr) {
+    if (!dbg.ensure(fs * 6 + lr_bytes)) {
       c.err = "device allocation failed";
       return DVC_E_NOMEM;
     }
     specs[0].dbg_si_initial = dbg.as<uint8_t>();
     specs[0].dbg_si_final = dbg.as<uint8_t>() + fs;
     specs[0].dbg_alpha = (float *)(dbg.as<uint8_t>() + 2 * fs);
+    if (dbg_lr) specs[0].dbg_lr = (float *)(dbg.as<uint8_t>() + 6 * fs);
   }
   std::vector<dvc::FrameResult> res;
   if (!ctx->batcher.decode(c, specs, res, s)) return c.err.find("alloc") != std::string::npos ? DVC_E_NOMEM : DVC_E_CUDA;
@@ -307,6 +434,9 @@ static int decode_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames, uint8_t 
   if (dbg_alpha &&
       (st = cuda_status(c, cudaMemcpyAsync(dbg_alpha, dbg.as<uint8_t>() + 2 * fs, fs * 4, cudaMemcpyDeviceToHost, s),
                         "D2H dbg")))
+    return st;
+  if (dbg_lr && (st = cuda_status(c, cudaMemcpyAsync(dbg_lr, dbg.as<uint8_t>() + 6 * fs, lr_bytes,
+                                                      cudaMemcpyDeviceToHost, s), "D2H dbg")))
     return st;
   if ((st = cuda_status(c, cudaStreamSynchronize(s), "decode sync"))) return st;
   for (int i = 0; i < count; i++) {

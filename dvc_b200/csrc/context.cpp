@@ -60,9 +60,11 @@ bool Context::init(const char *data, const char *tables, int dev) {
   mkdir(table_dir.c_str(), 0755);
   if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return false;
   if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
-  // process-wide, set by every context creation (1024 unless the variable asks for 512)
+  // process-wide, set by every context creation: CIF 1024 unless the variable
+  // asks for 512, QCIF 256 unless it asks for 512 or 1024
   const char *nt = getenv("DVC_LDPCA_THREADS");
-  set_ldpca_threads(nt ? atoi(nt) : 1024);
+  const char *ntq = getenv("DVC_LDPCA_THREADS_QCIF");
+  set_ldpca_threads(nt ? atoi(nt) : 1024, ntq ? atoi(ntq) : 256);
 
   // library-exact math tables: load, or sweep the C library once and cache
   const std::string xpath = table_dir + "/xlm_tables.bin";
@@ -130,6 +132,9 @@ bool Context::init(const char *data, const char *tables, int dev) {
     phi_bytes = (pk.desc.size() + pk.rec.size() + pk.val.size()) * 4;
   }
 
+  if (!near_ties.ensure(8) || !cuda_ok(cudaMemset(near_ties.p, 0, 8), "near-tie counter"))
+    return fail("device allocation failed");
+
   // LDPCA ladders (QCIF n=1584 and CIF n=6336)
   const std::string lpath = data_dir + "/ldpca_ladders.bin";
   if (!file_exists(lpath)) return fail("missing ladder file " + lpath);
@@ -155,6 +160,8 @@ void Context::release() {
   ld_res.release();
   ld_ent.release();
   ld_jobs.release();
+  near_ties.release();
+  for (DevBuf *b : {&bt_lr, &bt_acc, &bt_dec, &bt_res, &bt_ent, &bt_cw, &bt_state}) b->release();
   if (stream) cudaStreamDestroy(stream);
   stream = nullptr;
 }

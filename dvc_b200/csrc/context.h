@@ -38,6 +38,11 @@ struct Context {
   cudaStream_t stream = nullptr;
   // scratch for the batched LDPCA entry point
   DevBuf ld_lr, ld_acc, ld_dec, ld_res, ld_ent, ld_jobs;
+  // buffers of the batched LDPCA entry point (dvc_ldpca_decode_batch)
+  DevBuf bt_lr, bt_acc, bt_dec, bt_res, bt_ent, bt_cw, bt_state;
+  // count of reconstruction steps near a rounding tie (recon_kernel), one
+  // unsigned 64-bit word, zeroed at set-up
+  DevBuf near_ties;
 
   bool init(const char *data_dir, const char *table_dir, int device);
   void release();

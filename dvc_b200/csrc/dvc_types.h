@@ -2,6 +2,8 @@
 #pragma once
 #include <stdint.h>
 
+#include "libm_tables.h"
+
 namespace dvc {
 
 // LDPCA ladder for one codeword length, resident in device memory.
@@ -54,6 +56,45 @@ struct LdpcaJob {
 struct LdpcaSpec {
   int *best = nullptr, *iters = nullptr, *start = nullptr, *done = nullptr, *slot_code = nullptr;
   uint8_t *slot_dec = nullptr;
+};
+
+// Batched form (k_ldpca_batch.cu): one codeword of a mixed-length batch.
+struct LdpcaBatchCw {
+  int cif;          // 1: n = 6336 (CIF ladder), 0: n = 1584 (QCIF ladder)
+  int crc;          // CRC-8 of the source bits
+  int given_start;  // first ladder code to try, or -1: the conditional-entropy bound picks it
+  long long lr_off, acc_off, dec_off;  // offsets of its LRs (floats), accumulated syndrome and decoded bits (bytes)
+};
+
+// Ladder state of one codeword of a batch.
+struct LdpcaBatchState {
+  int start;                 // first code
+  int best;                  // lowest code that succeeded so far (LDPCA_NONE: none)
+  int fin;                   // 1 once a group has been elected to finalise the codeword
+  int nsucc;                 // successes so far (each takes the next slot)
+  unsigned long long mask;   // bit c - start: code c has finished
+  int succ_code[4];          // code that filled each slot
+  int iters[64];             // BP iterations of code start + k
+};
+
+// Arguments of the batched launch (all device pointers).
+struct LdpcaBatch {
+  LadderDev L_cif, L_qcif;
+  XlmDev xt;
+  const LdpcaBatchCw *cw;
+  LdpcaBatchState *state;
+  uint32_t *slot_bits;       // [count * 4 * 198] packed decoded bits of successes
+  const float *lr;
+  const uint8_t *acc;
+  uint8_t *decoded;          // may be null
+  int *results;              // [count * 4] rate, first code, accepted code, BP iterations of the ladder
+  float *entropy;            // [count] conditional-entropy bound, may be null
+  const int *cif, *qcif;     // indices of the CIF and of the QCIF codewords
+  int n_cif, n_qcif;
+  int last_cif, last_qcif;   // full-rate code index of each ladder
+  int *ctr;                  // [2] queue heads (CIF, QCIF), zeroed before the launch
+  unsigned long long *work;  // BP iterations run, abandoned and skipped-over codes included
+  int max_iter;
 };
 
 }  // namespace dvc

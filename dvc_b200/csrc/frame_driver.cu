@@ -214,6 +214,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     D.ifc = (double)(F.future_idx - F.cur_idx) / (double)(F.future_idx - F.past_idx);
     D.ipc = (double)(F.cur_idx - F.past_idx) / (double)(F.future_idx - F.past_idx);
     D.active = 1;
+    D.near_ties = ctx.near_ties.as<unsigned long long>();
     int level_shift[16] = {0};
     for (int j = 1; j < 16; j++)
       if (kQTable[q][j] > 0) level_shift[j] = (kQTable[q][j] - 2) / 2;
@@ -330,6 +331,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
 
   // LDPCA jobs for every step
   LdpcaJob *jobs = (LdpcaJob *)(pin + jobs_off);
+  plane_of_.assign(steps.size() * nf, -1);
   for (size_t si = 0; si < steps.size(); si++) {
     const int band = steps[si].band, bit = steps[si].bit, index = kZigzag[band];
     for (int f = 0; f < nf; f++) {
@@ -340,6 +342,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
       for (int b = 0; b <= band; b++) coded = coded && kQBits[q][kZigzag[b]] > 0;
       if (!coded || bit > kQBits[q][index]) continue;
       const int plane = plane_base[f][band] + (kQBits[q][index] - bit);
+      plane_of_[si * nf + f] = plane;
       Slot &S = slots_[f];
       J.active = 1;
       J.lr = fd[f].lr;
@@ -444,6 +447,14 @@ bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileSt
     for (; si < steps.size() && steps[si].band == band; si++) {
       if (!ctx.cuda_ok(launch_cond_bit(fdev, nf, w, h, band, steps[si].bit, s), "conditional bit probability"))
         return false;
+      for (int f = 0; f < nf; f++)
+        if (frames[f].dbg_lr && plane_of_[si * nf + f] >= 0) {
+          const size_t n = (size_t)w * h / 16;
+          if (!ctx.cuda_ok(cudaMemcpyAsync(frames[f].dbg_lr + (size_t)plane_of_[si * nf + f] * n, fd[f].lr, n * 4,
+                                           cudaMemcpyDeviceToDevice, s),
+                           "debug copy"))
+            return false;
+        }
       if (prof) cudaEventRecord(ev_[ev_used_], s);
       if (!ctx.cuda_ok(launch_ldpca_spec(*L, jobs_dev_.as<LdpcaJob>() + si * nf, nf, ctx.xlm, max_iter, spec_k_,
                                          ldpca_spec_carve(spec_.p, nf, spec_k_), s),

@@ -38,6 +38,7 @@ struct FrameSpec {
   uint8_t *dbg_si_initial = nullptr;  // side information after createSideInfo + intra copy
   float *dbg_alpha = nullptr;         // noise parameters
   uint8_t *dbg_si_final = nullptr;    // side information after the last refinement
+  float *dbg_lr = nullptr;            // [qbits * w*h/16] condBitProb likelihood ratios of every bitplane
 };
 
 struct FrameResult {
@@ -107,6 +108,7 @@ class FrameBatcher {
   std::vector<Step> steps_;
   std::vector<FrameDev> fd_;
   std::vector<int> qb_, wz_bits0_;
+  std::vector<int> plane_of_;  // [step * frames + frame]: the frame's bitplane decoded at that step, or -1
   std::vector<const FrameSpec *> specs_;
   std::vector<FrameSpec> spec_copy_;
   int nf_ = 0, w_ = 0, h_ = 0, max_nsir_ = 0;

@@ -35,6 +35,9 @@ struct FrameDev {
   const uint8_t *past_mode;   // [w*h/64]
   uint8_t *db_img, *db_mode;  // [w*h] filtered copy; [2*w*h/16] edge mode (vertical edges, then horizontal)
   double *db_bs;              // [2*w*h/16] edge strength
+  // reconstruction steps whose rounding could depend on the last bits of exp
+  // (counted by recon_kernel; null: not counted)
+  unsigned long long *near_ties;
   int active;                 // 0: the descriptor is a placeholder, every kernel skips it
 };
 

@@ -57,6 +57,11 @@ __device__ __forceinline__ bool in_step(const FrameDev &F, int band, int bit) {
 // ROUND, defines.h:23
 __device__ __forceinline__ int dround(double x) { return x >= 0.0 ? (int)(x + 0.5) : -(int)(-x + 0.5); }
 
+// x moved by k units in the last place (x positive and finite)
+__device__ __forceinline__ double ulp_shift(double x, int k) {
+  return __longlong_as_double(__double_as_longlong(x) + (long long)k);
+}
+
 // costFunc, sideInfoCreation.cpp:10-12 (K is the float 0.05f, promoted)
 __device__ __forceinline__ double cost_func(double mad, double vx, double vy) {
   return mad * (1.0 + (double)0.05f * sqrt(vx * vx + vy * vy));
@@ -839,17 +844,32 @@ __global__ void recon_kernel(FrameDev *frames, int band) {
     const int sc = F.side_trans[ci];
     const double a = F.alpha[ci];
     int v;
+    // The reference rounds with its C library's double exp; this kernel uses
+    // the device's.  Both are within an ulp of the true value, and every other
+    // operation here is IEEE and identical on both sides, so the rounded result
+    // can only differ where moving an exp result by a couple of ulps moves the
+    // argument of ROUND across a .5 boundary.  Such steps are counted (every
+    // exp result moved by -2 and +2 ulps), so a decode can show that it met none.
+    bool tie = false;
     if (a <= 0.0001) {
       v = (lo + hi) / 2;
-    } else if (sc < lo) {
-      v = lo + dround(1.0 / a + (double)step / (1.0 - exp(a * (double)step)));
-    } else if (sc >= hi) {
-      v = hi - dround(1.0 / a + (double)step / (1.0 - exp(a * (double)step)));
+    } else if (sc < lo || sc >= hi) {
+      const double e = exp(a * (double)step);
+      const int u = dround(1.0 / a + (double)step / (1.0 - e));
+      for (int k = -2; k <= 2 && F.near_ties; k += 4)
+        tie |= dround(1.0 / a + (double)step / (1.0 - ulp_shift(e, k))) != u;
+      v = sc < lo ? lo + u : hi - u;
     } else {
       const double r = sc - lo, d = hi - sc;
       const double er = exp(-a * r), ed = exp(-a * d);
-      v = sc + dround(((r + 1.0 / a) * er - (d + 1.0 / a) * ed) / (2.0 - (er + ed)));
+      const int u = dround(((r + 1.0 / a) * er - (d + 1.0 / a) * ed) / (2.0 - (er + ed)));
+      for (int k = 0; k < 4 && F.near_ties; k++) {
+        const double er2 = ulp_shift(er, (k & 1) ? 2 : -2), ed2 = ulp_shift(ed, (k & 2) ? 2 : -2);
+        tie |= dround(((r + 1.0 / a) * er2 - (d + 1.0 / a) * ed2) / (2.0 - (er2 + ed2))) != u;
+      }
+      v = sc + u;
     }
+    if (tie) atomicAdd(F.near_ties, 1ull);
     F.side_trans[ci] = v;
     F.dbf[ci] = ((v ^ sc) != 0) ? 1 : 0;
   }

@@ -25,25 +25,8 @@
 //    are identical to the sequential ladder while idle SMs shorten it, with one
 //    launch per bitplane step.
 //
-// Edge messages are kept in row order (each row's edges contiguous, in
-// increasing edge index), so a row sum is a sequential pass over contiguous
-// shared memory in the reference's summation order; columns (every column has
-// degree 3) reach their edges through the per-code position array.  The
-// parity check of an iteration's hard decision is folded into the next row
-// pass.  The magnitude phi(y) = -logf(tanhf(y)) is one record read of the
-// packed table (dvc_common.cuh; its hot part stays in L2), and the reads of a
-// pass are issued in batches so that several are in flight per thread.  Shared
-// memory is kept under 132 KB so that the rest of the SM's 256 KB stays L1
-// cache for the per-code position arrays and the table records that
-// successive iterations read again.
-//
-// Shared memory per codeword (n bits, e edges; CIF n=6336, e=19008: 124 KB):
-//   msg[e]  f32  edge messages by row-order position, in place:
-//                phi(|v->c|) -> c->v -> next phi(|v->c|)
-//   rowt[n] f32  row sums (after decoding: the decoded bits, one byte each)
-//   sgd[e]  u8   bit 0: sign of the v->c message, bit 1: hard decision of its column
-//   rpar[n] u8   bit 0: syndrome bit of the row, bit 1: sign parity of the row
-// The log-LRs of a thread's columns stay in registers.
+// The per-code BP, the syndrome, the inverse and the shared-memory layout are
+// in ldpca_bp.cuh.
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -51,147 +34,43 @@
 #include "dvc_common.cuh"
 #include "dvc_types.h"
 #include "kernels.h"
+#include "ldpca_bp.cuh"
 
 namespace dvc {
 
-#define LDPCA_LOG2 (0.693147181f)  // LdpcaDecoder.cpp:18
-#define LDPCA_NONE 0x7f7f7f7f      // "no success yet" (memset pattern 0x7f)
-
-// largest codeword length; each thread keeps the log-LRs of up to
-// LDPCA_MAX_N / NT columns in registers
-#define LDPCA_MAX_N 6336
-
-static __host__ __device__ size_t ldpca_smem_bytes(int n, int e) {
-  size_t b = (size_t)e * 4;  // msg
-  b += (size_t)n * 4;        // rowt
-  b += (size_t)e;            // sgd
-  b += (size_t)n;            // rpar
-  return (b + 15) & ~(size_t)15;
-}
-
 size_t ldpca_smem_size(int n, int e) { return ldpca_smem_bytes(n, e); }
 
-// fused bitplane insertion (putBitplaneToCoeff, bitplane.cpp:4-22)
-__device__ __forceinline__ void put_bitplane(const LdpcaJob &J, const uint8_t *dec, int n) {
-  const int b4w = J.w >> 2, b8w = J.w >> 3;
-  const int row = J.index_in_blk >> 2, col = J.index_in_blk & 3;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    const int i = k / b4w, j = k - i * b4w;
-    if (J.mode[(i >> 1) * b8w + (j >> 1)] == DVC_WZ_B) {
-      int *p = J.recons_trans + ((i << 2) + row) * J.w + (j << 2) + col;
-      *p = (*p << 1) + (int)dec[k];
-    }
-  }
-}
-
-// decoded = inv(H) * syndrome of the full-rate code (LdpcaDecoder.cpp:695-716);
-// syndrome words are built in `sw` (n/32 words of shared memory)
-__device__ void invh_decode(const LadderDev &L, const uint8_t *synd, uint8_t *dec, uint32_t *sw) {
-  const int n = L.n, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nt = blockDim.x;
-  for (int base = warp * 32; base < n; base += nt) {
-    const int k = base + lane;
-    const uint32_t b = __ballot_sync(0xffffffffu, k < n && (synd[k] & 1));
-    if (lane == 0) sw[base >> 5] = b;
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < n; j += nt) {
-    const uint32_t *row = L.invh + (size_t)j * L.invh_words;
-    uint32_t x = 0;
-    for (int w = 0; w < L.invh_words; w++) x ^= __ldg(row + w) & sw[w];
-    dec[j] = (uint8_t)(__popc(x) & 1);
-  }
-  __syncthreads();
-}
-
-// syndrome of ladder code `code` from the accumulated syndrome bits (LdpcaDecoder.cpp:684-693)
-__device__ __forceinline__ void build_syndrome(const LadderDev &L, int code, const uint8_t *acc, uint8_t *synd) {
-  const int m = L.synd_len[code], nb = L.bpp[code];
-  const int *idx = L.idx + (size_t)code * L.period;
-  for (int k = threadIdx.x; k < m; k += blockDim.x) {
-    uint8_t s = acc[idx[k % nb] + (k / nb) * L.period];
-    if (k > 0) s ^= acc[idx[(k - 1) % nb] + ((k - 1) / nb) * L.period];
-    synd[k] = s;
-  }
-}
-
-// the same from the packed accumulated-syndrome bytes (MSB first, ByteToBit)
-__device__ __forceinline__ uint8_t acc_bit(const uint8_t *packed, int i) {
-  return (uint8_t)((__ldg(packed + (i >> 3)) >> (7 - (i & 7))) & 1);
-}
-__device__ __forceinline__ void build_syndrome_packed(const LadderDev &L, int code, const uint8_t *packed,
-                                                      uint8_t *synd) {
-  const int m = L.synd_len[code], nb = L.bpp[code];
-  const int *idx = L.idx + (size_t)code * L.period;
-  for (int k = threadIdx.x; k < m; k += blockDim.x) {
-    uint8_t s = acc_bit(packed, idx[k % nb] + (k / nb) * L.period);
-    if (k > 0) s ^= acc_bit(packed, idx[(k - 1) % nb] + ((k - 1) / nb) * L.period);
-    synd[k] = s;
-  }
-}
-
-template <int NT>
-__global__ void __launch_bounds__(NT, 1)
+// One thread block of NT threads per (codeword, speculative slot), each thread
+// holding MAXC = ceil(n / NT) columns.  By default NT = 1024 for CIF codewords
+// (one block per SM: 124 KB of shared memory) and NT = 256 for QCIF ones
+// (31 KB each, four blocks per SM).
+template <int NT, int MAXC>
+__global__ void __launch_bounds__(NT, 1024 / NT)
     ldpca_ladder_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, XlmDev xt, int max_iter, int K,
                         LdpcaSpec sp) {
-  constexpr int MAXC = (LDPCA_MAX_N + NT - 1) / NT;  // columns per thread
-  constexpr int UNR = 8;                             // edge-pass table reads in flight per thread
-  constexpr int CB = NT >= 1024 ? 1 : 4;             // column-pass columns per batch (3 reads each)
   extern __shared__ __align__(16) uint8_t smem[];
   const int j = blockIdx.x / K, kk = blockIdx.x - j * K;
   const LdpcaJob J = jobs[j];
   if (!J.active) return;
   const bool spec = sp.best != nullptr;
-  const int n = L.n, E = L.e, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  float *msg = reinterpret_cast<float *>(smem);
-  float *rowt = msg + E;
-  uint8_t *sgd = reinterpret_cast<uint8_t *>(rowt + n);
-  uint8_t *rpar = sgd + E;
-  uint8_t *dec = reinterpret_cast<uint8_t *>(rowt);  // decoded bits, once BP is over
+  const LdGroup<NT, true> g{(int)threadIdx.x, 0};
+  const int n = L.n, tid = threadIdx.x;
+  const LdSmem S = ld_carve(smem, n, L.e);
   __shared__ uint32_t s_ured[NT / 32];
   __shared__ int s_start, s_accepted, s_stop;
   __shared__ uint4 s_pdesc[XL_PHI_MAX_BINADES];
   const XlSmall xs = xl_small_global(xt);
   xl_phi_stage(xt, s_pdesc);
 
-  // accumulated syndrome bits (ByteToBit, LdpcaDecoder.cpp:81-107), entropy
-  // terms H_k = (P(-log P + log(1-P)) - log(1-P)) / LOG2 with P = LR/(1+LR)
-  // (ComputeCE), and log LR (LdpcaDecoder.cpp:665-666)
+  // accumulated syndrome bits (ByteToBit, LdpcaDecoder.cpp:81-107), log LR and
+  // the entropy terms (ComputeCE), the bound as a sequential sum in block order
   float llr[MAXC];
-#pragma unroll
-  for (int c = 0; c < MAXC; c++) {
-    const int k = tid + c * NT;
-    llr[c] = 0.0f;
-    if (k < n) {
-      const float lr = J.lr[k];
-      const float pco = lr / (1.0f + lr);
-      const float tmp = xl_logf(xt, xs, 1.0f - pco);
-      msg[k] = (pco * (-xl_logf(xt, xs, pco) + tmp) - tmp) / LDPCA_LOG2;
-      llr[c] = xl_logf(xt, xs, lr);
-      if (J.llr_out && kk == 0) J.llr_out[k] = llr[c];
-    }
-  }
-  __syncthreads();
+  ld_llr(g, n, J.lr, xt, xs, llr, S.msg, (J.llr_out && kk == 0) ? J.llr_out : nullptr);
+  g.sync();
   if (tid == 0) {
-    // the bound is a sequential float sum in block order
-    float h = 0.0f;
-    int k = 0;
-    for (; k + 8 <= n; k += 8) {
-      const float v0 = msg[k], v1 = msg[k + 1], v2 = msg[k + 2], v3 = msg[k + 3];
-      const float v4 = msg[k + 4], v5 = msg[k + 5], v6 = msg[k + 6], v7 = msg[k + 7];
-      h += v0;
-      h += v1;
-      h += v2;
-      h += v3;
-      h += v4;
-      h += v5;
-      h += v6;
-      h += v7;
-    }
-    for (; k < n; k++) h += msg[k];
-    h /= (float)n;
+    float h = ld_entropy_sum(S.msg, n);
     if (J.use_given_entropy) h = J.given_entropy;
-    int start = 0;
-    while (start < L.num_codes - 1 && L.code_rate[start] < h) start++;
+    const int start = ld_start_code(L, h);
     s_start = start;
     s_accepted = L.num_codes - 1;
     if (kk == 0) {
@@ -199,7 +78,7 @@ __global__ void __launch_bounds__(NT, 1)
       if (spec) sp.start[j] = start;
     }
   }
-  __syncthreads();
+  g.sync();
   const int start = s_start;
   const int last = L.num_codes - 1;
   int total_iters = 0;
@@ -208,156 +87,18 @@ __global__ void __launch_bounds__(NT, 1)
   for (int code = start + kk; code < last; code += K) {
     if (spec) {
       if (tid == 0) s_stop = *bestp < code;
-      __syncthreads();
+      g.sync();
       if (s_stop) break;
     }
-    const int m = L.synd_len[code];
-    const uint16_t *__restrict__ pos = L.pos + (size_t)code * E;
-    const uint16_t *__restrict__ rid = L.rid + (size_t)code * E;
-    build_syndrome_packed(L, code, J.acc, rpar);
-    __syncthreads();
-    const int *rp = L.row_ptr + (size_t)code * (n + 1);
-    // first magnitudes: phi(|LLR|) on the three edges of each column
-    {
-      float ph[MAXC];
-#pragma unroll
-      for (int c = 0; c < MAXC; c++)
-        ph[c] = tid + c * NT < n ? xl_phi(xt, s_pdesc, (fabsf(llr[c]) + 1e-9f) / 2.0f) : 0.0f;
-#pragma unroll
-      for (int c = 0; c < MAXC; c++) {
-        const int k = tid + c * NT;
-        if (k < n) {
-          const uint8_t ng = (uint8_t)(__float_as_uint(llr[c]) >> 31);
-#pragma unroll
-          for (int i = 0; i < 3; i++) {
-            const int p = __ldg(pos + 3 * k + i);
-            msg[p] = ph[c];
-            sgd[p] = ng;
-          }
-        }
-      }
-    }
-    __syncthreads();
-    bool converged = false;
     int it = 0;
-    for (;;) {
-      // (R) rows: sum of the magnitudes in edge order and the sign parity with
-      //     the syndrome bit, for the next edge pass; from the second pass on
-      //     also the parity check of the previous hard decision
-      int wrong = 0;
-      for (int r = tid; r < m; r += NT) {
-        const int p0 = rp[r], p1 = rp[r + 1];
-        float s = 0.0f;
-        uint32_t x = 0;  // bit 0: xor of signs, bit 1: xor of decisions
-        for (int p = p0; p < p1; p++) {
-          s += msg[p];
-          x ^= sgd[p];
-        }
-        const uint32_t syn = rpar[r] & 1u;
-        rowt[r] = s;
-        rpar[r] = (uint8_t)(syn | (((x & 1u) ^ syn) << 1));
-        wrong |= (int)(((x >> 1) ^ syn) & 1u);
-      }
-      if (spec && tid == 0) s_stop = *bestp < code;
-      const int any_wrong = __syncthreads_or(wrong);
-      if (it > 0 && !any_wrong) {
-        converged = true;
-        break;
-      }
-      // abandon a code above a known success
-      if (it == max_iter || (spec && s_stop)) break;
-      it++;
-      // (E) edges: c->v = phi(row sum - own magnitude) with the product of
-      //     the other signs
-      for (int p0 = tid; p0 < E; p0 += UNR * NT) {
-        float c[UNR];
-        int rr[UNR];
-#pragma unroll
-        for (int q = 0; q < UNR; q++) {
-          // lanes past the last edge repeat it (no branch, so that the UNR
-          // table reads are in flight together) and store nothing
-          const int p = min(p0 + q * NT, E - 1);
-          rr[q] = __ldg(rid + p);
-          c[q] = xl_phi(xt, s_pdesc, (rowt[rr[q]] - msg[p] + 1e-9f) / 2.0f);
-        }
-#pragma unroll
-        for (int q = 0; q < UNR; q++) {
-          const int p = p0 + q * NT;
-          if (p < E) msg[p] = c[q] * ((((uint32_t)rpar[rr[q]] >> 1) ^ (sgd[p] & 1u)) ? -1.0f : 1.0f);
-        }
-      }
-      __syncthreads();
-      // (C) columns: total in edge order, hard decision, extrinsic messages
-      //     and their magnitudes for the next iteration
-#pragma unroll
-      for (int c0 = 0; c0 < MAXC; c0 += CB) {
-        float ph[CB][3];
-        uint32_t sb[CB][3];
-        int pp[CB][3];
-#pragma unroll
-        for (int b = 0; b < CB; b++) {
-          const int c = c0 + b, k = tid + c * NT;
-          if (c < MAXC && k < n) {
-            float mv[3];
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-              pp[b][i] = __ldg(pos + 3 * k + i);
-              mv[i] = msg[pp[b][i]];
-            }
-            float tmp = llr[c];
-            tmp += mv[0];
-            tmp += mv[1];
-            tmp += mv[2];
-            const uint32_t d = __float_as_uint(tmp) >> 31;
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-              const float v = tmp - mv[i];
-              sb[b][i] = (__float_as_uint(v) >> 31) | (d << 1);
-              ph[b][i] = xl_phi(xt, s_pdesc, (fabsf(v) + 1e-9f) / 2.0f);
-            }
-          }
-        }
-#pragma unroll
-        for (int b = 0; b < CB; b++) {
-          const int c = c0 + b, k = tid + c * NT;
-          if (c < MAXC && k < n)
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-              msg[pp[b][i]] = ph[b][i];
-              sgd[pp[b][i]] = (uint8_t)sb[b][i];
-            }
-        }
-      }
-      __syncthreads();
-    }
+    const int ok = ld_try_code(g, L, code, llr, J.acc, J.crc, xt, s_pdesc, max_iter, bestp, S, s_ured, &s_stop, it);
     total_iters += it;
-    if (!converged) continue;
-    // hard decision of each column (bit 1 of its edges' sgd) into dec, and the
-    // CRC-8 of the decoded bitplane as the xor of single-bit CRCs (the CRC is
-    // linear for a fixed length with zero initial value and no final xor)
-    uint32_t c = 0;
-    for (int k = tid; k < n; k += NT) {
-      const uint8_t d = (uint8_t)((sgd[__ldg(pos + 3 * k)] >> 1) & 1u);
-      dec[k] = d;
-      if (d) c ^= __ldg(L.crc_tab + k);
-    }
-    for (int o = 16; o > 0; o >>= 1) c ^= __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) s_ured[warp] = c;
-    __syncthreads();
-    if (tid == 0) {
-      uint32_t t = 0;
-      for (int w = 0; w < NT / 32; w++) t ^= s_ured[w];
-      s_ured[0] = t;
-    }
-    __syncthreads();
-    const bool ok = (int)(s_ured[0] & 0xffu) == J.crc;
-    __syncthreads();
     if (ok) {
       if (tid == 0) s_accepted = code;
       if (spec) {
         uint8_t *slot = sp.slot_dec + (size_t)blockIdx.x * n;
-        for (int k = tid; k < n; k += NT) slot[k] = dec[k];
-        __syncthreads();
+        for (int k = tid; k < n; k += NT) slot[k] = S.dec[k];
+        g.sync();
         if (tid == 0) {
           sp.slot_code[blockIdx.x] = code;
           __threadfence();
@@ -373,13 +114,13 @@ __global__ void __launch_bounds__(NT, 1)
     // succeeded), then puts the codeword's scratch back to its initial state
     // for the next launch (no memset between the steps of a batch)
     __shared__ int s_slot, s_iters;
-    __syncthreads();
+    g.sync();
     if (tid == 0) {
       atomicAdd(sp.iters + j, total_iters);
       __threadfence();
       s_stop = atomicAdd(sp.done + j, 1) == K - 1;
     }
-    __syncthreads();
+    g.sync();
     if (!s_stop) return;
     __threadfence();
     if (tid == 0) {
@@ -395,10 +136,10 @@ __global__ void __launch_bounds__(NT, 1)
       s_slot = slot;
       s_iters = __ldcg(sp.iters + j);
     }
-    __syncthreads();
+    g.sync();
     if (s_slot >= 0) {
       const uint8_t *src = sp.slot_dec + (size_t)(j * K + s_slot) * n;
-      for (int k = tid; k < n; k += NT) dec[k] = __ldcg(src + k);
+      for (int k = tid; k < n; k += NT) S.dec[k] = __ldcg(src + k);
     }
     total_iters = s_iters;
     for (int k = tid; k < K; k += NT) sp.slot_code[j * K + k] = -1;
@@ -408,12 +149,12 @@ __global__ void __launch_bounds__(NT, 1)
       sp.done[j] = 0;
     }
   }
-  __syncthreads();
+  g.sync();
   const int accepted = s_accepted;
   if (accepted == last) {
-    build_syndrome_packed(L, last, J.acc, rpar);
-    __syncthreads();
-    invh_decode(L, rpar, dec, reinterpret_cast<uint32_t *>(msg));
+    ld_build_syndrome(g, L, last, J.acc, S.rpar);
+    g.sync();
+    ld_invh_decode(g, L, S.rpar, S.dec, reinterpret_cast<uint32_t *>(S.msg));
   }
   if (tid == 0) {
     J.result[0] = L.synd_len[accepted] + 8;
@@ -422,47 +163,63 @@ __global__ void __launch_bounds__(NT, 1)
     J.result[3] = total_iters;
   }
   if (J.decoded)
-    for (int k = tid; k < n; k += NT) J.decoded[k] = dec[k];
-  if (J.recons_trans) put_bitplane(J, dec, n);
+    for (int k = tid; k < n; k += NT) J.decoded[k] = S.dec[k];
+  if (J.recons_trans) ld_put_bitplane(g, J, S.dec, n);
 }
 
-template <int NT>
+template <int NT, int MAXC>
 static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_jobs, const XlmDev &xt, int max_iter,
                              int K, const LdpcaSpec &sp, cudaStream_t stream) {
-  if (L.n > LDPCA_MAX_N) return cudaErrorInvalidValue;
+  if (L.n > LDPCA_MAX_N || LDPCA_COLS(L.n, NT) > MAXC) return cudaErrorInvalidValue;
   const size_t smem = ldpca_smem_bytes(L.n, L.e);
-  // the attribute is per device: set it once for each device
+  // the attributes are per device: set them once for each device
   static std::atomic<uint64_t> attr_set{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   const uint64_t bit = 1ull << (dev & 63);
   if (!(attr_set.load() & bit)) {
-    const size_t most = ldpca_smem_bytes(LDPCA_MAX_N, 3 * LDPCA_MAX_N);
-    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most);
+    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT, MAXC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    // the smallest shared-memory split that holds one block, so that the rest
-    // of the SM's 256 KB is L1 for the phi records, which BP iterations re-read
-    // (percent of the 228 KB maximum; the driver rounds up to a supported split)
-    const int pct = (int)(((most + 4096) * 100 + 228 * 1024 - 1) / (228 * 1024));
-    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    // the smallest shared-memory split that holds the blocks an SM can run
+    // (1024 / NT of them), so that the rest of the SM's 256 KB is L1 for the
+    // phi records, which BP iterations re-read (percent of the 228 KB maximum;
+    // the driver rounds up to a supported split)
+    const size_t need = (size_t)(1024 / NT) * (smem + 4096);
+    const int pct = (int)((need * 100 + 228 * 1024 - 1) / (228 * 1024));
+    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT, MAXC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             pct > 100 ? 100 : pct);
     if (e != cudaSuccess) return e;
     attr_set.fetch_or(bit);
   }
-  ldpca_ladder_kernel<NT><<<num_jobs * K, NT, smem, stream>>>(L, jobs, xt, max_iter, K, sp);
+  ldpca_ladder_kernel<NT, MAXC><<<num_jobs * K, NT, smem, stream>>>(L, jobs, xt, max_iter, K, sp);
   return cudaGetLastError();
 }
 
-static int g_ldpca_threads = 1024;
+// threads per codeword block: CIF 1024 (or 512), QCIF 256 (or 512, 1024)
+static int g_ldpca_threads = 1024, g_ldpca_threads_qcif = 256;
 
-void set_ldpca_threads(int nt) { g_ldpca_threads = (nt == 512) ? 512 : 1024; }
+void set_ldpca_threads(int nt, int nt_qcif) {
+  g_ldpca_threads = (nt == 512) ? 512 : 1024;
+  g_ldpca_threads_qcif = (nt_qcif == 512 || nt_qcif == 1024) ? nt_qcif : 256;
+}
+
+static cudaError_t launch_shape(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
+                                int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream) {
+  if (L.n == 1584) {
+    if (g_ldpca_threads_qcif == 1024) return launch_nt<1024, 2>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+    if (g_ldpca_threads_qcif == 512) return launch_nt<512, 4>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+    return launch_nt<256, 7>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+  }
+  if (g_ldpca_threads == 512) return launch_nt<512, 13>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+  return launch_nt<1024, 7>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+}
 
 cudaError_t launch_ldpca(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt, int max_iter,
                          cudaStream_t stream) {
   if (num_jobs <= 0) return cudaSuccess;
   LdpcaSpec none{};
-  return g_ldpca_threads == 512 ? launch_nt<512>(L, jobs_dev, num_jobs, xt, max_iter, 1, none, stream)
-                                : launch_nt<1024>(L, jobs_dev, num_jobs, xt, max_iter, 1, none, stream);
+  return launch_shape(L, jobs_dev, num_jobs, xt, max_iter, 1, none, stream);
 }
 
 size_t ldpca_spec_scratch_bytes(int n, int num_jobs, int K) {
@@ -497,8 +254,7 @@ cudaError_t ldpca_spec_reset(const LdpcaSpec &sp, int num_jobs, int K, cudaStrea
 cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
                               int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream) {
   if (num_jobs <= 0) return cudaSuccess;
-  return g_ldpca_threads == 512 ? launch_nt<512>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream)
-                                : launch_nt<1024>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+  return launch_shape(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
 }
 
 }  // namespace dvc

@@ -20,7 +20,13 @@ LdpcaSpec ldpca_spec_carve(void *base, int num_jobs, int K);
 cudaError_t ldpca_spec_reset(const LdpcaSpec &sp, int num_jobs, int K, cudaStream_t stream);
 cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
                               int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream);
-void set_ldpca_threads(int nt);
+// threads per codeword block of the ladder kernel: CIF 1024 or 512, QCIF 256,
+// 512 or 1024 (other values select the defaults, 1024 and 256)
+void set_ldpca_threads(int nt, int nt_qcif);
+// batched form: one persistent launch over codewords of both lengths
+// (k_ldpca_batch.cu); state + slot bytes per codeword from ldpca_batch_state_bytes
+size_t ldpca_batch_state_bytes(int count);
+cudaError_t launch_ldpca_batch(LdpcaBatch A, int count, int grid, cudaStream_t stream);
 // encoder: accumulated syndromes (n/8 bytes, MSB first) and CRC-8 of `count` source bitplanes
 cudaError_t launch_ldpca_encode(const LadderDev &L, const uint8_t *bits_dev, int count, uint8_t *acc_dev,
                                 uint8_t *crc_dev, cudaStream_t stream);

@@ -47,7 +47,7 @@ def decode_levels(stream, start=0, end=None):
 
 
 def decode_sequence(ctx, stream, key_frames, ori_frames=None, key_bits=None, key_psnr=None, intra_bitstream=None):
-    """Decode every WZ frame. Returns dict(recon, bits, psnr, planes, deblock_flag).
+    """Decode every WZ frame. Returns dict(recon, bits, psnr, planes, entropy, deblock_flag).
 
     intra_bitstream: bytes of the sequence's intra bitstream, needed when frames
     have intra blocks (IntraMode 1); their pixels are decoded first
@@ -57,7 +57,7 @@ def decode_sequence(ctx, stream, key_frames, ori_frames=None, key_bits=None, key
     recon = np.array(key_frames, np.uint8, copy=True)
     bits = dict(key_bits or {})
     ps = dict(key_psnr or {})
-    planes, dbf = {}, {}
+    planes, dbf, entropy = {}, {}, {}
     intra_px = {}
     if any(fr.intra_mode for fr in stream.frames.values()):
         if intra_bitstream is None:
@@ -77,7 +77,8 @@ def decode_sequence(ctx, stream, key_frames, ori_frames=None, key_bits=None, key
             recon[m] = o["recon"]
             bits[m] = fr.skip_bits + fr.intra_map_bits + o["wz_bits"] + (intra_px[m][1] if m in intra_px else 0)
             planes[m] = o["planes"]
+            entropy[m] = o["entropy"]
             dbf[m] = o["deblock_flag"]
             if ori_frames is not None:
                 ps[m] = psnr(recon[m], ori_frames[m])
-    return dict(recon=recon, bits=bits, psnr=ps, planes=planes, deblock_flag=dbf)
+    return dict(recon=recon, bits=bits, psnr=ps, planes=planes, entropy=entropy, deblock_flag=dbf)

@@ -20,7 +20,7 @@ position ``idx[k % bpp] + (k // bpp) * period`` is >= the full-rate row of e
 the shipped QCIF decoder ladder exactly before writing anything.
 
 Usage (needs the reference tree; the output is committed):
-    python dvc_b200/ladders/make_ladders.py /root/reference
+    python dvc_b200/ladders/make_ladders.py <reference tree>
 """
 import os
 import struct
@@ -65,4 +65,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_ladders.py <reference tree>")
+    main(sys.argv[1])

@@ -95,6 +95,11 @@ FRAME_API = {
     "dvc_ldpca_decode_noalloc": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int, C.c_void_p],
     "dvc_debug_wz_frame": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p, C.c_void_p, C.c_void_p],
+    "dvc_debug_wz_frame_lr": [C.c_void_p, C.POINTER(WZFrame), C.c_void_p],
+    "dvc_ldpca_decode_batch": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_longlong),
+                               C.POINTER(C.c_double)],
+    "dvc_recon_near_ties": [C.c_void_p, C.POINTER(C.c_longlong)],
     "dvc_ldpca_encode": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p],
     "dvc_phi_table_check": [C.POINTER(C.c_size_t), C.c_char_p, C.c_int],
     "dvc_jbig_encode_mode_map": [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)],
@@ -165,6 +170,32 @@ class Context:
         self.check(lib().dvc_ldpca_decode(self._h, n, count, _ptr(lr), _ptr(acc), _ptr(crc), _ptr(dec), _ptr(res),
                                           _ptr(ent), max_iter))
         return dec, res, ent
+
+    def ldpca_decode_batch(self, lengths, lr, acc, crc, start=None, max_iter=50, want_decoded=True):
+        """dvc_ldpca_decode_batch: codewords of mixed lengths in one persistent launch.
+
+        lengths: int per codeword (1584 or 6336); lr: float32 LRs of all
+        codewords concatenated; acc: accumulated-syndrome bytes concatenated
+        (n/8 each); crc: uint8 per codeword; start: first ladder code per
+        codeword, or None for the entropy bound.  Returns (decoded bits
+        concatenated or None, results [count, 4], entropy [count], BP iterations
+        run, kernel milliseconds)."""
+        n = np.ascontiguousarray(lengths, np.int32)
+        count = len(n)
+        lr = np.ascontiguousarray(lr, np.float32)
+        acc = np.ascontiguousarray(acc, np.uint8)
+        crc = np.ascontiguousarray(crc, np.uint8)
+        assert lr.size == int(n.sum()) and acc.size == int(n.sum()) // 8 and crc.size == count
+        st = None if start is None else np.ascontiguousarray(start, np.int32)
+        dec = np.zeros(int(n.sum()), np.uint8) if want_decoded else None
+        res = np.zeros((count, 4), np.int32)
+        ent = np.zeros(count, np.float32)
+        work = C.c_longlong(0)
+        ms = C.c_double(0)
+        self.check(lib().dvc_ldpca_decode_batch(self._h, count, _ptr(n), _ptr(lr), _ptr(acc), _ptr(crc), _ptr(st),
+                                                _ptr(dec), _ptr(res), _ptr(ent), max_iter, C.byref(work),
+                                                C.byref(ms)))
+        return dec, res, ent, work.value, ms.value
 
     def ldpca_decode_noalloc(self, n, count, d_lr, d_acc, d_crc, d_decoded, d_results, d_entropy, max_iter=50,
                              stream=0):
@@ -244,6 +275,17 @@ class Context:
         """One frame through dvc_debug_wz_frame: the decode result plus si_initial, alpha, si_final."""
         return self.decode_wz_frames([item], debug=True)[0]
 
+    def debug_wz_frame_lr(self, item):
+        """One frame through dvc_debug_wz_frame_lr: the decode result plus "lr",
+        the likelihood ratios of every bitplane ([qbits, w*h/16] float32)."""
+        return self.decode_wz_frames([item], debug="lr")[0]
+
+    def recon_near_ties(self):
+        """dvc_recon_near_ties: reconstruction steps so far whose rounding could depend on exp's last bits."""
+        n = C.c_longlong(0)
+        self.check(lib().dvc_recon_near_ties(self._h, C.byref(n)))
+        return n.value
+
     def decode_wz_frames(self, items, debug=False):
         """Decode independent WZ frames as one batch.
 
@@ -276,7 +318,12 @@ class Context:
                              _ptr(crc), _ptr(acc), _ptr(rec), 0, _ptr(planes), _ptr(ent), _ptr(dbf),
                              it.get("deblock", 0), it.get("intra_qp", 0), _ptr(pmode))
             outs.append(dict(recon=rec, planes=planes, entropy=ent, deblock_flag=dbf))
-        if debug:
+        if debug == "lr":
+            w, h = items[0]["width"], items[0]["height"]
+            lr = np.zeros((len(items[0]["crc"]), w * h // 16), np.float32)
+            self.check(lib().dvc_debug_wz_frame_lr(self._h, arr, _ptr(lr)))
+            outs[0]["lr"] = lr
+        elif debug:
             w, h = items[0]["width"], items[0]["height"]
             si0 = np.zeros((h, w), np.uint8)
             si1 = np.zeros((h, w), np.uint8)

@@ -36,8 +36,9 @@ typedef struct dvc_ctx dvc_ctx;
  * forwardME_kernel.h:11, motionLearning_kernel.h:11; called at main.cpp:92-103).
  * Launch shape of the LDPCA ladder kernel, from the environment (the values
  * dvc_b200.autotune chooses by measurement; decoded output never depends on
- * them): DVC_LDPCA_THREADS = 512 or 1024 threads per codeword block (default
- * 1024), read here; DVC_LDPCA_SPEC_FLOOR = 1..32, the least number of
+ * them): DVC_LDPCA_THREADS = 512 or 1024 threads per CIF codeword block
+ * (default 1024) and DVC_LDPCA_THREADS_QCIF = 256, 512 or 1024 per QCIF
+ * codeword block (default 256), read here; DVC_LDPCA_SPEC_FLOOR = 1..32, the least number of
  * speculative blocks per codeword in a frame batch (default 8), and
  * DVC_LDPCA_SPEC = 1..32, a fixed number instead, both read when a batch is
  * prepared. */
@@ -182,6 +183,49 @@ int dvc_decode_wz_frames(dvc_ctx *ctx, int count, dvc_wz_frame *frames);
  * last updateSI (:318).  No counterpart in the reference. */
 int dvc_debug_wz_frame(dvc_ctx *ctx, dvc_wz_frame *frame, uint8_t *si_initial, float *alpha, uint8_t *si_final);
 
+/* dvc_decode_wz_frames on one frame that also returns the likelihood ratios
+ * p0/p1 of every bitplane as condBitProb computes them (noiseModel.cpp:191-310,
+ * called at DVC_Decoder.cpp:210) and LdpcaDecoder receives them:
+ * lr_planes[qbits][w*h/16], bitplanes in decoding order (band by band in
+ * zig-zag order, most significant bit first), QbitsNumPerBlk bitplanes for the
+ * frame's QIndex.  No counterpart in the reference. */
+int dvc_debug_wz_frame_lr(dvc_ctx *ctx, dvc_wz_frame *frame, float *lr_planes);
+
+/* Reconstruction steps (reconstruction.cpp:184-289) met so far on this
+ * context's device whose rounding ROUND(x) could change if an exp result
+ * differed by up to 2 units in the last place: the reference calls its C
+ * library's double exp there and the device its own, so a count of 0 shows
+ * that no decoded coefficient can depend on that difference.  No counterpart
+ * in the reference. */
+int dvc_recon_near_ties(dvc_ctx *ctx, long long *count);
+
+/* Batched LDPCA decode of `count` codewords of mixed lengths in one
+ * persistent launch (the batching form of the decoder): every codeword walks
+ * the rate-adaptive ladder from its own start level, and the device schedules
+ * (codeword, ladder code) pairs over all SMs from a work queue, so that
+ * codewords of uneven length and request level share the GPU without
+ * lockstep.  Results equal LdpcaDecoder's (LdpcaDecoder.cpp:646-771) for each
+ * codeword with RateLowerBound = the rate of its start code.
+ *   n[count]            codeword lengths, 1584 or 6336, in any order
+ *   lr[sum n]           p0/p1 of every codeword, concatenated in order
+ *   acc[sum n / 8]      accumulated syndrome bytes, MSB first, concatenated
+ *   crc[count]          CRC-8 of each source codeword
+ *   start[count]        first ladder code to try (0..64), or NULL: the
+ *                       conditional-entropy bound picks it (ComputeCE)
+ *   decoded[sum n]      out: decoded bits, concatenated (may be NULL)
+ *   results[count*4]    out: rate (m+8), first code, accepted code, and the BP
+ *                       iterations the sequential ladder runs
+ *   entropy[count]      out: conditional-entropy bound (may be NULL)
+ *   max_iter            BP iterations per ladder code (the reference uses 50)
+ *   bp_iterations       out: BP iterations the launch ran, codes abandoned
+ *                       above an earlier success included (may be NULL)
+ *   kernel_ms           out: device time of the launch (may be NULL)
+ * Replaces, for many codewords at once, the per-request host loop of
+ * beliefPropagation_CUDA_earlyJump (LDPCA_cuda.cu:872-969). */
+int dvc_ldpca_decode_batch(dvc_ctx *ctx, int count, const int *n, const float *lr, const uint8_t *acc,
+                           const uint8_t *crc, const int *start, uint8_t *decoded, int *results, float *entropy,
+                           int max_iter, long long *bp_iterations, double *kernel_ms);
+
 /* Most codewords one dvc_ldpca_decode_noalloc call accepts. */
 #define DVC_NOALLOC_MAX_CODEWORDS 1024
 
@@ -195,8 +239,12 @@ int dvc_debug_wz_frame(dvc_ctx *ctx, dvc_wz_frame *frame, uint8_t *si_initial, f
  * library's device memory (DVC_NOALLOC_MAX_CODEWORDS entries, about 100 KB,
  * held on every GPU that loads the library until the process exits); more
  * codewords per call are rejected with DVC_E_ARG.  The first call on each
- * device looks that array's address up, so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race.
+ * device sets that device up: it looks the array's address up, sets the LDPCA
+ * kernel's shared-memory attributes and loads the kernels' module, so make it
+ * before any stream capture.  The address is kept for the life of the process,
+ * so a device reset (cudaDeviceReset) while the library is loaded is not
+ * supported by this entry point.  All calls share the array: calls that
+ * overlap on the GPU race.
  *   d_lr[count*n] f32, d_acc[count*n/8], d_crc[count]       inputs
  *   d_decoded[count*n] (may be NULL), d_results[count*4],    outputs
  *   d_entropy[count] (may be NULL)

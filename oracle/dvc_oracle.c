@@ -212,6 +212,13 @@ static void invh_mul(const dvco_ladder *L, uint8_t *decoded, const uint8_t *synd
 /* LdpcaDecoder, LdpcaDecoder.cpp:646-771 (ParallelMode 0 branch). */
 int dvco_ldpca_decode(const dvco_ladder *L, float *lr, const uint8_t *acc, uint8_t *decoded, int *rate,
                       uint8_t crc, float entropy, int *start_code) {
+  return dvco_ldpca_decode_iter(L, lr, acc, decoded, rate, crc, entropy, start_code, MAX_ITERATIONS);
+}
+
+/* The same with another cap on BP iterations per ladder code (the reference's
+ * is the compile-time MAX_ITERATIONS, 50). */
+int dvco_ldpca_decode_iter(const dvco_ladder *L, float *lr, const uint8_t *acc, uint8_t *decoded, int *rate,
+                           uint8_t crc, float entropy, int *start_code, int max_iter) {
   const int n = L->n;
   int start = 0;
   while (start < L->num_codes - 1 &&
@@ -237,7 +244,7 @@ int dvco_ldpca_decode(const dvco_ladder *L, float *lr, const uint8_t *acc, uint8
       invh_mul(L, decoded, synd);
       break;
     }
-    if (dvco_belief_propagation(L, lr, synd, decoded, m, code, MAX_ITERATIONS, NULL)) {
+    if (dvco_belief_propagation(L, lr, synd, decoded, m, code, max_iter, NULL)) {
       if (dvco_crc8_bits(decoded, n) == crc) break;
     }
   }

@@ -36,6 +36,10 @@ typedef struct {
 int dvco_ldpca_decode(const dvco_ladder *L, float *lr, const uint8_t *acc_bits, uint8_t *decoded,
                       int *rate, uint8_t crc, float entropy, int *start_code);
 
+/* dvco_ldpca_decode with max_iter BP iterations per ladder code instead of 50. */
+int dvco_ldpca_decode_iter(const dvco_ladder *L, float *lr, const uint8_t *acc_bits, uint8_t *decoded,
+                           int *rate, uint8_t crc, float entropy, int *start_code, int max_iter);
+
 /* Sum-product BP on one code (LdpcaDecoder.cpp:462-580); returns 1 if all
  * parity checks hold within max_iter iterations. *iters gets the iteration count. */
 int dvco_belief_propagation(const dvco_ladder *L, const float *llr, const uint8_t *syndrome,

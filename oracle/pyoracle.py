@@ -47,6 +47,7 @@ def lib():
             raise FileNotFoundError(LIB_PATH + " (run make -C oracle oracle)")
         _lib = C.CDLL(LIB_PATH)
         _lib.dvco_ldpca_decode.restype = C.c_int
+        _lib.dvco_ldpca_decode_iter.restype = C.c_int
         _lib.dvco_compute_ce.restype = C.c_float
         _lib.dvco_compute_ce.argtypes = [C.c_void_p, C.c_int]
         _lib.dvco_crc8_bits.restype = C.c_uint8
@@ -94,15 +95,16 @@ class OracleLadder:
         return cls._cache[n]
 
 
-def ldpca_decode(ladder, lr, acc_bits, crc, entropy):
-    """One LdpcaDecoder call. Returns (decoded bits, rate, start code, accepted code, log-LR)."""
+def ldpca_decode(ladder, lr, acc_bits, crc, entropy, max_iter=50):
+    """One LdpcaDecoder call (max_iter BP iterations per code; the reference's
+    cap is 50). Returns (decoded bits, rate, start code, accepted code, log-LR)."""
     lr = np.ascontiguousarray(lr, np.float32).copy()
     acc = np.ascontiguousarray(acc_bits, np.uint8)
     dec = np.zeros(ladder.n, np.uint8)
     rate = C.c_int(0)
     start = C.c_int(0)
-    acc_code = lib().dvco_ldpca_decode(C.byref(ladder.c), _p(lr), _p(acc), _p(dec), C.byref(rate),
-                                       C.c_uint8(crc), C.c_float(entropy), C.byref(start))
+    acc_code = lib().dvco_ldpca_decode_iter(C.byref(ladder.c), _p(lr), _p(acc), _p(dec), C.byref(rate),
+                                            C.c_uint8(crc), C.c_float(entropy), C.byref(start), max_iter)
     return dec, rate.value, start.value, acc_code, lr
 
 

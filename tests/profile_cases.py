@@ -1,8 +1,9 @@
-"""Small, self-contained GPU workloads for profiler captures.
+"""Small, self-contained GPU workloads for profiler captures (not a test module).
 
-    python -m dvc_b200.profile_cases ldpca-cif     # LDPCA ladder on the 11 CIF golden bitplanes
-    python -m dvc_b200.profile_cases frame-cif [Q] # one CIF WZ frame (QIndex Q, default 4) through every kernel
-    python -m dvc_b200.profile_cases ldpca-micro   # 148 CIF codewords of the LDPCA microbenchmark, one launch
+    python tests/profile_cases.py ldpca-cif     # LDPCA ladder on the CIF golden bitplanes
+    python tests/profile_cases.py frame-cif [Q] # one CIF WZ frame (QIndex Q, default 4) through every kernel
+    python tests/profile_cases.py ldpca-micro   # 148 CIF codewords of the LDPCA microbenchmark, one launch
+    python tests/profile_cases.py ldpca-batch [N] # N codewords (default 1024) of the batched workload, one launch
 
 Each case runs once after one warm-up run, so a profiler can skip the warm-up
 launches and capture the second instance of a kernel.
@@ -13,6 +14,7 @@ import sys
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
 
 
 def ldpca_cif(ctx):
@@ -23,7 +25,7 @@ def ldpca_cif(ctx):
 
 
 def frame_cif(ctx, q=4):
-    from . import bitstream as bs, decoder, encoder, synth
+    from dvc_b200 import bitstream as bs, decoder, encoder, synth
     ori, key = synth.make_sequence("cif", 3, 101)
     st = bs.parse_wz(encoder.encode_sequence(ori, 2, q))
     m, b, e = bs.sequence_order(st.n_frames, st.gop)[0]
@@ -33,7 +35,7 @@ def frame_cif(ctx, q=4):
 
 
 def ldpca_micro(ctx, count=148):
-    from . import ldpca_bench as lb
+    from dvc_b200 import ldpca_bench as lb
     lr, acc, crc, x = lb.make_codewords(6336, count, 5)
     for _ in range(2):
         dec, res, ent = ctx.ldpca_decode(lr, acc, crc)
@@ -41,11 +43,19 @@ def ldpca_micro(ctx, count=148):
     print("bp block-iterations per launch", int(res[:, 3].sum()))
 
 
-CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif, "ldpca-micro": ldpca_micro}
+def ldpca_batch(ctx, count=1024):
+    from dvc_b200 import ldpca_bench as lb
+    n, lr, acc, crc, start, src, where = lb.interleaved(count, 11)
+    for _ in range(2):
+        dec, res, ent, work, ms = ctx.ldpca_decode_batch(n, lr, acc, crc, start, 50)
+    print("codewords", count, "kernel ms", ms, "bp iterations", work)
+
+
+CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif, "ldpca-micro": ldpca_micro, "ldpca-batch": ldpca_batch}
 
 
 def main():
-    from . import native
+    from dvc_b200 import native
     name = sys.argv[1] if len(sys.argv) > 1 else "ldpca-cif"
     ctx = native.Context(0)
     CASES[name](ctx, *[int(a) for a in sys.argv[2:]])

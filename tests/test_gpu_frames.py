@@ -15,13 +15,21 @@ pytestmark = pytest.mark.gpu
                                  "qcif_g4_q8_allintra", "qcif_g2_q4_full", "cif_g4_q6_full",
                                  "qcif_still_g4_q4_full", "cif_g4_q4_own_full", "qcif_g2_q8_own_full",
                                  "qcif_still_g4_q4_own_full", "cif_fast_g8_q8_own_full",
-                                 "cif_fast_g8_q4_own_full", "qcif_g2_q4_db", "qcif_g4_q6_db"])
+                                 "cif_fast_g8_q4_own_full", "qcif_g2_q4_db", "qcif_g4_q6_db",
+                                 "cif_g2_q1_full", "cif_g4_q3_full", "cif_g2_q5_full", "cif_g4_q7_full",
+                                 "cif_g4_q8_full", "cif_g2_q8_wz", "qcif_g2_q4_cfg0"])
 def test_sequence_matches_reference(gpu_ctx, golden_dir, seq):
+    """Every WZ frame of a reference-decoded sequence: decoded Y, bits and PSNR,
+    and per bitplane the first and accepted ladder codes and the bits of the
+    conditional-entropy bound; no reconstruction step may sit near a rounding
+    tie that the C library's exp and the device's could resolve differently."""
     g = np.load(os.path.join(golden_dir, f"seq_{seq}.npz"))
     ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
     st = bs.parse_wz(g["wz"].tobytes())
     intra_bs = g["intra"].tobytes() if "intra" in g.files else None
+    ties0 = gpu_ctx.recon_near_ties()
     res = decoder.decode_sequence(gpu_ctx, st, key, ori, intra_bitstream=intra_bs)
+    assert gpu_ctx.recon_near_ties() == ties0, "a reconstruction step sat near a rounding tie"
     for f, b, p, wz in zip(g["frames"], g["bits"], g["psnr"], g["is_wz"]):
         if wz:
             f = int(f)
@@ -33,6 +41,42 @@ def test_sequence_matches_reference(gpu_ctx, golden_dir, seq):
     acc = np.concatenate([res["planes"][m][:, 2] for (m, _, _) in order])
     assert np.array_equal(start, g["ld_start"])
     assert np.array_equal(acc, g["ld_accepted"])
+    ent = np.concatenate([res["entropy"][m] for (m, _, _) in order]).astype(np.float32)
+    assert np.array_equal(ent.view(np.uint32), g["ld_entropy"].astype(np.float32).view(np.uint32)), \
+        "conditional-entropy bounds differ"
+
+
+def _digest64(a):
+    import hashlib
+    return int.from_bytes(hashlib.blake2b(np.ascontiguousarray(a).tobytes(), digest_size=8).digest(), "little")
+
+
+@pytest.mark.parametrize("seq", ["qcif_g2_q4", "cif_g2_q2", "qcif_g2_q4_full", "cif_g2_q5_full", "cif_g2_q8_wz",
+                                 "cif_g4_q7_full", "qcif_g2_q4_cfg0"])
+def test_first_frame_likelihood_ratios_match_reference(gpu_ctx, golden_dir, seq):
+    """The likelihood ratios of every bitplane of the first decoded WZ frame
+    (condBitProb's output, the LDPCA decoder's input) against the ones the
+    reference passed to its LdpcaDecoder: bit for bit (a digest per bitplane;
+    the first bitplanes are stored in full and also checked to 1e-6 relative,
+    so that a failure shows the size of the difference)."""
+    from dvc_b200 import intra
+    g = np.load(os.path.join(golden_dir, f"seq_{seq}.npz"))
+    ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
+    st = bs.parse_wz(g["wz"].tobytes())
+    m, b, e = bs.sequence_order(st.n_frames, st.gop)[0]
+    recon = np.array(key, np.uint8, copy=True)
+    if st.frames[m].intra_mode:
+        recon[m] = intra.decode_all(st, g["intra"].tobytes(), recon)[m][0]
+    out = gpu_ctx.debug_wz_frame_lr(decoder.frame_item(st, st.frames[m], recon))
+    lr = out["lr"]
+    head = g["lr0_head"]
+    assert lr.shape[0] == len(g["lr0_hash"])
+    rel = np.abs(lr[:len(head)].astype(np.float64) - head) / np.maximum(np.abs(head.astype(np.float64)), 1e-30)
+    assert rel.max() <= 1e-6, "likelihood ratio off by %g relative" % rel.max()
+    assert np.array_equal(lr[:len(head)].view(np.uint32), head.view(np.uint32)), "likelihood ratios differ in bits"
+    got = np.array([_digest64(x) for x in lr], np.uint64)
+    bad = np.nonzero(got != g["lr0_hash"])[0]
+    assert len(bad) == 0, "likelihood ratios of bitplanes %s differ" % bad.tolist()
 
 
 @pytest.mark.parametrize("seq", ["qcif_g2_q4", "cif_g2_q2"])

@@ -39,3 +39,21 @@ def test_device_encoder_matches_host_encoder_and_round_trips(gpu_ctx, n):
     assert np.array_equal(crc_dev, crc_host)
     dec, res, ent = gpu_ctx.ldpca_decode(lr, acc_dev, crc_dev)
     assert np.array_equal(dec, x)
+
+
+@pytest.mark.parametrize("k", range(6))
+def test_full_rate_inverse_matches_reference(gpu_ctx, golden_dir, k):
+    """Codewords no ladder code below full rate decodes (QCIF and CIF): the
+    reference ends at its GF(2) inverse (LdpcaDecoder.cpp:695-716), rate N + 8;
+    the device ladder must reach the same code and the same decoded bits, with
+    the entropy bound (which picks the first code) equal in bits."""
+    g = np.load(os.path.join(golden_dir, "ldpca_fullrate.npz"))
+    n = int(g["c%d_n" % k])
+    lr = g["c%d_lr" % k][None]
+    acc = g["c%d_acc" % k][None]
+    crc = np.array([g["c%d_crc" % k]], np.uint8)
+    dec, res, ent = gpu_ctx.ldpca_decode(lr, acc, crc, max_iter=50)
+    assert np.float32(ent[0]).view(np.uint32) == np.float32(g["c%d_entropy" % k]).view(np.uint32)
+    assert res[0, 0] == int(g["c%d_rate" % k]) == n + 8
+    assert res[0, 2] == 64
+    assert np.array_equal(dec[0], g["c%d_decoded" % k])

@@ -175,3 +175,54 @@ def test_oracle_cif_intra_deblocked_frame_matches_reference(golden_dir):
     qb = len(res["planes"][m][0])
     assert np.array_equal(res["planes"][m][0], g["ld_start"][:qb])
     assert np.array_equal(res["planes"][m][1], g["ld_accepted"][:qb])
+
+
+def test_oracle_config0_sequence_matches_reference(golden_dir):
+    """The reference's plain CPU run (QCIF, 17 frames, GOP 2, QIndex 4, every
+    option off) through the oracle: pixels, rates, PSNR and ladder codes."""
+    test_oracle_sequence_matches_reference(golden_dir, "qcif_g2_q4_cfg0")
+
+
+@pytest.mark.parametrize("k", [4, 5])
+def test_oracle_full_rate_matches_reference(golden_dir, k):
+    """QCIF codewords that only the GF(2) inverse decodes: the oracle's ladder
+    walks every code to full rate as the reference's did."""
+    g = load(golden_dir, "ldpca_fullrate.npz")
+    n = int(g["c%d_n" % k])
+    L = po.OracleLadder.get(n)
+    lr = g["c%d_lr" % k]
+    ent = po.compute_ce(lr)
+    assert np.float32(ent) == g["c%d_entropy" % k]
+    acc_bits = np.unpackbits(g["c%d_acc" % k], bitorder="big")[:n]
+    dec, rate, start, acc_code, _ = po.ldpca_decode(L, lr, acc_bits, int(g["c%d_crc" % k]), ent)
+    assert rate == int(g["c%d_rate" % k]) == n + 8 and acc_code == 64
+    assert np.array_equal(dec, g["c%d_decoded" % k])
+
+
+def _digest64(a):
+    import hashlib
+    return int.from_bytes(hashlib.blake2b(np.ascontiguousarray(a).tobytes(), digest_size=8).digest(), "little")
+
+
+@pytest.mark.parametrize("n,count", [(1584, 24), (6336, 6)])
+def test_oracle_batch_codewords_match_reference(golden_dir, n, count):
+    """The first codewords of the batched LDPCA workload (dvc_b200.ldpca_bench:
+    seeded sources, flip probabilities and start levels): the generator
+    reproduces the inputs the reference decoded, and the oracle started at each
+    codeword's seeded level reaches the reference's rate and decoded bits."""
+    from dvc_b200 import ldpca_bench as lb
+    g = load(golden_dir, "ldpca_batch.npz")
+    half = int(g["count"]) // 2
+    seed = int(g["seed"]) + n
+    lr, acc, crc, x = lb.make_codewords(n, half, seed)
+    assert [_digest64(lr), _digest64(acc), _digest64(crc)] == [int(v) for v in g["n%d_input_hash" % n]]
+    starts = lb.seeded_starts(n, half, seed)
+    assert np.array_equal(starts, g["n%d_start" % n])
+    rates = lb.code_rates(n)
+    L = po.OracleLadder.get(n)
+    for i in range(count):
+        bits = np.unpackbits(acc[i], bitorder="big")[:n]
+        dec, rate, start, acc_code, _ = po.ldpca_decode(L, lr[i], bits, int(crc[i]), float(rates[starts[i]]))
+        assert start == starts[i]
+        assert rate == g["n%d_rate" % n][i]
+        assert _digest64(dec) == int(g["n%d_decoded_hash" % n][i])
