@@ -49,7 +49,7 @@ def encode(yuv, key_yuv, n_frames, size, gop, qindex, skip=0, intra=0, intra_qp=
 
 
 def decode(ori_yuv, wz, intra_bs, key_yuv, stat, mode=0, cores=1, capture=None, capture_pdf=False,
-           start=None, end=None, frame_rate=15, binary="DvcDec", timeout=None):
+           start=None, end=None, frame_rate=15, binary="DvcDec", timeout=None, env_extra=None):
     """Run the reference decoder in its own cwd.
 
     Returns dict(rd=<RD text>, yuv=<bytes of the Y-only output>, stdout=..., seconds=wall).
@@ -62,6 +62,7 @@ def decode(ori_yuv, wz, intra_bs, key_yuv, stat, mode=0, cores=1, capture=None, 
                 f'KeyFrameInfo = "{stat}"\nRDFile = "rd"\nOutputSequences = "dec"\nFrameRate = {frame_rate}\n'
                 f'ParallelMode = {mode}\nUseCoreNum = {cores}\nIntraBitstream = "{intra_bs}"\n')
     env = dict(os.environ)
+    env.update(env_extra or {})
     if capture:
         env["DVC_CAPTURE"] = capture
         binary = "DvcDec_capture"

@@ -36,6 +36,8 @@ bytes (``lr0_hash``) and the first bitplanes in full (``lr0_head``).
                    codewords, half of each length, seeded flip probability and
                    start level): per codeword the reference LdpcaDecoder's rate
                    and a digest of its decoded bits (oracle/ldpca_ref.cpp).
+  ranges.npz       the reference decoder run with -startFrame/-endFrame on
+                   committed sequences: its decoded luma and RD report.
   ldpca_fullrate.npz codewords so noisy that no ladder code below full rate
                    decodes them, so the reference ends at the GF(2) inverse
                    (LdpcaDecoder.cpp:695-716): LR, accumulated syndrome, CRC,
@@ -386,6 +388,38 @@ def bench_first_gops_fixture(pool, tmp):
     np.savez_compressed(os.path.join(HERE, "bench_first_gops.npz"), **out)
 
 
+RANGES = [("qcif_g2_q4_full", 2, 4), ("qcif_g2_q4_full", 0, 2), ("cif_g4_q3_full", 4, 8),
+          ("qcif_g2_q4_cfg0", 6, 12)]
+
+
+def range_fixture(tmp):
+    """The reference decoder run with -startFrame/-endFrame on committed
+    sequences (main.cpp:118-142: skipGOP replays the intra bitstream of the
+    GOPs before the start; frame.cpp:99-103: the decoded luma ends one frame
+    before endFrame unless endFrame is the sequence's last frame): its decoded
+    luma file and RD report per range."""
+    out = {}
+    for k, (name, a, b) in enumerate(RANGES):
+        g = np.load(os.path.join(HERE, "seq_%s.npz" % name))
+        ori, key = synth.make_sequence(str(g["kind"]), int(g["n_frames"]), int(g["seed"]))
+        d = os.path.join(tmp, "range%d" % k)
+        os.makedirs(d, exist_ok=True)
+        oy, ky, st = os.path.join(d, "ori.yuv"), os.path.join(d, "key.yuv"), os.path.join(d, "stat.txt")
+        synth.write_yuv420(oy, ori)
+        synth.write_yuv420(ky, key)
+        synth.write_frame_stat(st, int(g["n_frames"]))
+        wz, ib = os.path.join(d, "s.wz"), os.path.join(d, "s.intra")
+        g["wz"].tofile(wz)
+        g["intra"].tofile(ib)
+        r = refrun.decode(oy, wz, ib, ky, st, mode=0, start=a, end=b)
+        out["r%d_seq" % k] = name
+        out["r%d_start" % k] = a
+        out["r%d_end" % k] = b
+        out["r%d_yuv" % k] = np.frombuffer(r["yuv"], np.uint8)
+        out["r%d_rd" % k] = np.array(r["rd"])
+    np.savez_compressed(os.path.join(HERE, "ranges.npz"), count=len(RANGES), **out)
+
+
 def _sequence_job(name, args, tmp):
     recs, n = run(name, *args[:5], tmp, *args[5:])
     if name == "qcif_g4_q8":
@@ -418,6 +452,8 @@ def main():
             ldpca_fullrate_fixture(pool)
         if not want or "ldpca_batch" in want:
             ldpca_batch_fixture(pool)
+        if not want or "ranges" in want:
+            range_fixture(tmp)
         for f in futs:
             name, nb = f.result()
             print(name, "bitplanes", nb)

@@ -97,3 +97,32 @@ def test_cli_decodes_golden_sequence(tmp_path, golden_dir, seq):
         else:
             assert "(KY)" in line
     assert any(x.startswith("Average WZ decoding speed:") for x in rd)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", range(4))
+def test_cli_frame_range_matches_reference(tmp_path, golden_dir, k):
+    """dvcdec -startFrame=a -endFrame=b against the reference decoder run with
+    the same flags (tests/golden/ranges.npz): the GOPs before the start only
+    advance the intra bitstream (skipGOP, DVC_Decoder.cpp:477-517), the RD
+    report lists frames a..b (frame.cpp:255-270) and the decoded luma holds
+    frames a..b, or a..b-1 when b is not the last frame (frame.cpp:99-103).
+    Every line of the report is compared except the timing figures."""
+    rg = np.load(os.path.join(golden_dir, "ranges.npz"))
+    seq, a, b = str(rg["r%d_seq" % k]), int(rg["r%d_start" % k]), int(rg["r%d_end" % k])
+    g = dict(np.load(os.path.join(golden_dir, f"seq_{seq}.npz")))
+    d, cfg = _setup(tmp_path, g)
+    r = subprocess.run([_cli(), "-d", cfg, "-GPUid=0", "-startFrame=%d" % a, "-endFrame=%d" % b],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert np.array_equal(np.fromfile(os.path.join(d, "dec.yuv"), np.uint8), rg["r%d_yuv" % k])
+
+    def stable(text):
+        out = []
+        for line in text.splitlines():
+            if line.startswith(("Total decoding time", "Average WZ decoding speed")):
+                continue
+            out.append(line.split(", Decoding time")[0])
+        return out
+
+    assert stable(open(os.path.join(d, "rd.txt")).read()) == stable(str(rg["r%d_rd" % k]))
