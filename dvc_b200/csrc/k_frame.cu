@@ -1327,9 +1327,24 @@ cudaError_t launch_deblock(FrameDev *fr, int nf, int w, int h, cudaStream_t s) {
 
 static inline dim3 g2(int n, int tpb, int frames) { return dim3((n + tpb - 1) / tpb, frames); }
 
+// threads per search block of the two motion searches (the candidate columns
+// or positions each thread walks follow from it); process-wide, set when a
+// context is created (dvc_b200.autotune picks them; the output never depends on them)
+static int g_si_threads = 128, g_fme_threads = 256;
+
+void set_me_shapes(int si_threads, int fme_threads) {
+  g_si_threads = (si_threads == 64 || si_threads == 256) ? si_threads : 128;
+  g_fme_threads = (fme_threads == 128 || fme_threads == 512) ? fme_threads : 256;
+}
+
 cudaError_t launch_side_info(FrameDev *fr, int nf, int w, int h, cudaStream_t s) {
   const int b16n = (w / 16) * (h / 16), b8n = (w / 8) * (h / 8);
-  forward_me_kernel<256><<<dim3(b16n, nf), 256, 0, s>>>(fr);
+  if (g_fme_threads == 128)
+    forward_me_kernel<128><<<dim3(b16n, nf), 128, 0, s>>>(fr);
+  else if (g_fme_threads == 512)
+    forward_me_kernel<512><<<dim3(b16n, nf), 512, 0, s>>>(fr);
+  else
+    forward_me_kernel<256><<<dim3(b16n, nf), 256, 0, s>>>(fr);
   forward_me_post_kernel<<<g2(b16n, 128, nf), 128, 0, s>>>(fr);
   bidirect_me_kernel<1024><<<nf, 1024, 0, s>>>(fr, 16);
   init_blk_mv_kernel<<<g2(b8n, 128, nf), 128, 0, s>>>(fr);
@@ -1368,7 +1383,12 @@ cudaError_t launch_band_end(FrameDev *fr, int nf, int w, int h, int max_nsir, in
                             cudaStream_t s) {
   if (max_nsir <= 0) return cudaSuccess;
   recon_kernel<<<g2(max_nsir, 128, nf), 128, 0, s>>>(fr, band);
-  update_si_kernel<128><<<dim3(max_nsir, nf), 128, 0, s>>>(fr, band);
+  if (g_si_threads == 64)
+    update_si_kernel<64><<<dim3(max_nsir, nf), 64, 0, s>>>(fr, band);
+  else if (g_si_threads == 256)
+    update_si_kernel<256><<<dim3(max_nsir, nf), 256, 0, s>>>(fr, band);
+  else
+    update_si_kernel<128><<<dim3(max_nsir, nf), 128, 0, s>>>(fr, band);
   over_complete_kernel<<<dim3((w - 3 + 127) / 128, nf, h - 3), 128, 0, s>>>(fr, band);
   update_smf_kernel<<<g2(max_nsir * 32, 128, nf), 128, 0, s>>>(fr, xt, band);
   update_ml_kernel<<<g2(max_nsir * 16, 128, nf), 128, 0, s>>>(fr, band);

@@ -23,6 +23,9 @@ cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int 
 // threads per codeword block of the ladder kernel: CIF 1024 or 512, QCIF 256,
 // 512 or 1024 (other values select the defaults, 1024 and 256)
 void set_ldpca_threads(int nt, int nt_qcif);
+// threads per search block of updateSI (64, 128 or 256) and of the forward
+// motion search (128, 256 or 512); other values select 128 and 256
+void set_me_shapes(int si_threads, int fme_threads);
 // batched form: one persistent launch over codewords of both lengths
 // (k_ldpca_batch.cu); state + slot bytes per codeword from ldpca_batch_state_bytes
 size_t ldpca_batch_state_bytes(int count);

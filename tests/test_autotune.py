@@ -1,4 +1,4 @@
-"""The LDPCA launch-shape autotuner's host logic (dvc_b200.autotune) on the CPU:
+"""The launch-shape autotuner's host logic (dvc_b200.autotune) on the CPU:
 the settings tried, the choice, the parity guard across settings, the saved
 file and its application, and the workload's cross-stream reference indices.
 The timing itself runs on a GPU (python -m dvc_b200.autotune)."""
@@ -25,7 +25,8 @@ def test_space_covers_threads_and_floors():
     s = at.space()
     assert len(s) == len(at.THREADS) * len(at.SPEC_FLOORS)
     assert {d[at.ENV_THREADS] for d in s} == {"512", "1024"}
-    assert {int(d[at.ENV_FLOOR]) for d in s} == set(at.SPEC_FLOORS)
+    assert {int(d[at.ENV_FLOOR]) for d in s} == {int(x) for x in at.SPEC_FLOORS}
+    assert all(set(d) == set(at.ENV_ALL) for d in s)
 
 
 def test_tune_picks_fastest_median_and_restores_env():
@@ -40,10 +41,28 @@ def test_tune_picks_fastest_median_and_restores_env():
         return [base + 5, base, base - 1, base + 50], fake_outputs(3, bp_seed=k)
 
     best, results = at.tune(measure, at.space(), env)
-    assert best["setting"] == {at.ENV_THREADS: "1024", at.ENV_FLOOR: "8"}
+    assert best["setting"] == dict(at.defaults(), **{at.ENV_THREADS: "1024", at.ENV_FLOOR: "8"})
     assert len(results) == len(at.space()) and len(seen) == len(results)
-    assert seen[0] == ("512", "1")
-    assert env == {at.ENV_FLOOR: "3"}  # restored: the variable set before, the other removed
+    assert seen[0] == ("1024", "1")
+    assert env == {at.ENV_FLOOR: "3"}  # restored: the variable set before, the others removed
+
+
+def test_coordinate_search_finds_each_knobs_best_value():
+    """A step time with a separate best value per knob: the coordinate search
+    reaches it, tries each setting once, and leaves the environment as it was."""
+    want = {at.ENV_THREADS: "1024", at.ENV_THREADS_QCIF: "512", at.ENV_FLOOR: "12", at.ENV_SI: "64",
+            at.ENV_FME: "512"}
+    env = {}
+
+    def measure(st):
+        assert all(env[k] == v for k, v in st.items())
+        t = 100.0 + sum(5.0 * (st[k] != v) + 0.0001 * int(st[k]) for k, v in want.items())
+        return [t, t + 1, t - 1], fake_outputs(2, bp_seed=len(st[at.ENV_FLOOR]))
+
+    best, results = at.tune_coordinates(measure, env=env)
+    assert best["setting"] == want
+    assert len(results) == 1 + sum(len(v) - 1 for _, v in at.KNOBS)
+    assert env == {}
 
 
 def test_tune_refuses_settings_that_decode_differently():
@@ -58,15 +77,17 @@ def test_tune_refuses_settings_that_decode_differently():
 
 
 def test_save_and_apply(tmp_path):
-    best = {"setting": {at.ENV_THREADS: "1024", at.ENV_FLOOR: "12"}, "ms": [3.0, 2.0, 4.0]}
+    best = {"setting": {at.ENV_THREADS: "1024", at.ENV_FLOOR: "12", at.ENV_SI: "64"}, "ms": [3.0, 2.0, 4.0]}
     p = tmp_path / "tuning.json"
     at.save(str(p), best, [best], "test device")
     doc = json.loads(p.read_text())
     assert doc["best"] == best["setting"] and doc["median_ms"] == 3.0 and doc["device"] == "test device"
     env = {}
-    assert at.apply(str(p), env) == {at.ENV_THREADS: "1024", at.ENV_FLOOR: "12"}
+    got = at.apply(str(p), env)
+    assert {k: v for k, v in got.items() if v is not None} == best["setting"]
     env = {at.ENV_FLOOR: "4"}  # a value the caller set wins
-    assert at.apply(str(p), env) == {at.ENV_THREADS: "1024", at.ENV_FLOOR: "4"}
+    got = at.apply(str(p), env)
+    assert got[at.ENV_FLOOR] == "4" and got[at.ENV_THREADS] == "1024" and got[at.ENV_SI] == "64"
 
 
 def test_workload_references_stay_within_each_stream():

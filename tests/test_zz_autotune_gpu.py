@@ -1,7 +1,7 @@
 """The autotuner's measurement on the device: a small batched CIF session decoded
-under three launch shapes of the LDPCA ladder (threads per codeword block and
-speculative-width floor), each a fresh context; tune() requires every shape
-to decode the same frames, rates and ladder codes."""
+under three launch shapes (threads per LDPCA codeword block, speculative-width
+floor, threads per updateSI and forward-search block), each a fresh context;
+tune() requires every shape to decode the same frames, rates and ladder codes."""
 import os
 
 import numpy as np
@@ -15,8 +15,10 @@ pytestmark = pytest.mark.gpu
 def test_launch_shapes_decode_identically():
     from dvc_b200 import native
     items = at.workload(n_streams=2, n_frames=9)
-    settings = [{at.ENV_THREADS: "1024", at.ENV_FLOOR: "8"}, {at.ENV_THREADS: "512", at.ENV_FLOOR: "1"},
-                {at.ENV_THREADS: "1024", at.ENV_FLOOR: "32"}]
+    base = at.defaults()
+    settings = [dict(base), dict(base, **{at.ENV_THREADS: "512", at.ENV_FLOOR: "1", at.ENV_SI: "64",
+                                          at.ENV_FME: "512"}),
+                dict(base, **{at.ENV_FLOOR: "32", at.ENV_SI: "256", at.ENV_FME: "128"})]
 
     def measure(setting):
         ctx = native.Context(0)
@@ -30,8 +32,8 @@ def test_launch_shapes_decode_identically():
         finally:
             ctx.close()
 
-    before = {k: os.environ.get(k) for k in (at.ENV_THREADS, at.ENV_FLOOR)}
+    before = {k: os.environ.get(k) for k in at.ENV_ALL}
     best, results = at.tune(measure, settings)
     assert len(results) == 3 and best["setting"] in settings
     assert all(np.isfinite(r["ms"]).all() and min(r["ms"]) > 0 for r in results)
-    assert {k: os.environ.get(k) for k in (at.ENV_THREADS, at.ENV_FLOOR)} == before
+    assert {k: os.environ.get(k) for k in at.ENV_ALL} == before
