@@ -28,6 +28,10 @@ Our arm prints one JSON line with:
   served  Poisson arrivals at fractions of the measured capacity through
           dvc_server (requests drawn from the first-level frames): throughput
           and per-frame latency p50/p99 (submit to completion);
+  served_mixed  the mixed serving workload (dvc_b200.serve_bench: 64 streams,
+          48 QCIF and 16 CIF, GOP 2/4/8, QIndex 1..8) at Poisson rates of
+          300, 1000 and 5000 frames/s, with the plain drop-in on the same
+          requests and a check that every served frame equals the plain one;
   plain   the one-frame-at-a-time drop-in (one dvc_decode_wz_frames call per
           frame) with per-frame latency p50/p99;
   roofline, cpu_baseline, clocks, gpu_launches.
@@ -374,6 +378,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed 64-stream serving workload")
     ap.add_argument("--max-batch", type=int, default=16)
     ap.add_argument("--streams", type=int, default=16)
     args = ap.parse_args()
@@ -492,6 +497,42 @@ def main():
     srv.close()
     served_main = served_sweep[2]
 
+    # the mixed serving workload: 64 streams (48 QCIF, 16 CIF), GOP 2/4/8,
+    # QIndex 1..8, Poisson arrivals, 16 GB budget (dvc_b200.serve_bench)
+    mixed = None
+    if not args.no_mixed:
+        from dvc_b200 import serve_bench as sb
+        t_build = time.perf_counter()
+        mreqs = sb.build(17)
+        t_build = time.perf_counter() - t_build
+        msrv = ctx.server(mem_budget_bytes=16 << 30, streams=args.streams, max_cohort=args.max_batch)
+        sb.serve(msrv, mreqs, np.zeros(len(mreqs)))  # warm
+        msweep = []
+        for rate in (300.0, 1000.0, 5000.0):
+            arr = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, len(mreqs)))
+            dt, lat, mserved = sb.serve(msrv, mreqs, arr)
+            msweep.append({"offered_rate": rate, "throughput": len(mreqs) / dt, "p50_ms": float(np.percentile(lat, 50)),
+                           "p99_ms": float(np.percentile(lat, 99))})
+        msrv.close()
+        # the plain drop-in on the same requests (one dvc_decode_wz_frames call each, in order)
+        pres, plat = {}, []
+        for k, it in enumerate(mreqs):
+            sub = {key: v for key, v in it.items() if not key.startswith("_")}
+            for name, d in zip(("past", "future"), (it["past_idx"], it["future_idx"])):
+                for dep in it["_deps"]:
+                    if mreqs[dep]["_frame"] == d:
+                        sub[name] = pres[dep]
+            t1 = time.perf_counter()
+            pres[k] = ctx.decode_wz_frames([sub])[0]["recon"]
+            plat.append(time.perf_counter() - t1)
+        mixed = {"workload": "64 streams (48 QCIF SkipBlock 0 IntraMode 0, 16 CIF SkipBlock 1 IntraMode 1 "
+                             "DeblockingFilter 1), GOP 2/4/8, QIndex 1..8, 17 frames each, Poisson arrivals, "
+                             "16 GB budget", "requests": len(mreqs), "sweep": msweep,
+                 "plain": {"throughput": len(mreqs) / sum(plat), "p50_ms": 1e3 * float(np.percentile(plat, 50)),
+                           "p99_ms": 1e3 * float(np.percentile(plat, 99))},
+                 "served_equals_plain": all(np.array_equal(mserved[k], pres[k]) for k in range(len(mreqs))),
+                 "build_s": t_build}
+
     # plain one-frame-at-a-time drop-in: one first-level frame per Q
     plain_lat = []
     for q in QS:
@@ -568,6 +609,7 @@ def main():
             "served": dict(served_main, unit="WZ frames/s",
                            arrivals="Poisson at 70% of the batched capacity, first-level frames",
                            streams=args.streams, max_cohort=args.max_batch, sweep=served_sweep),
+            "served_mixed": mixed,
             "roofline": {"bound": "hbm", "kernel": "ldpca_ladder_kernel", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                          "unit_of_work": "BP block-iteration on a CIF codeword, %d algorithmic bytes (phi-table "
