@@ -5,8 +5,8 @@
 Five launch parameters are chosen by measurement on the device the tuner runs on:
   - threads per CIF codeword block of the LDPCA ladder, 512 or 1024 (edges per
     thread = 19,008 / threads: 38 or 19; columns per thread 13 or 7);
-  - threads per QCIF codeword block, 256, 512 or 1024 (edges per thread 19, 10
-    or 5; four, two or one codewords per SM);
+  - threads per QCIF codeword block, 1024, 256 or 512 (edges per thread 5, 19
+    or 10; one, four or two codewords per SM);
   - the floor of the speculative ladder width: every codeword of a bitplane step
     is decoded by max(floor, SMs / codewords in flight) blocks, each starting at
     another code of the ladder (1 turns speculation off);
@@ -36,7 +36,7 @@ import numpy as np
 
 ENV_THREADS, ENV_THREADS_QCIF, ENV_FLOOR = "DVC_LDPCA_THREADS", "DVC_LDPCA_THREADS_QCIF", "DVC_LDPCA_SPEC_FLOOR"
 ENV_SI, ENV_FME = "DVC_SI_THREADS", "DVC_FME_THREADS"
-KNOBS = [(ENV_THREADS, ("1024", "512")), (ENV_THREADS_QCIF, ("256", "512", "1024")),
+KNOBS = [(ENV_THREADS, ("1024", "512")), (ENV_THREADS_QCIF, ("1024", "256", "512")),
          (ENV_FLOOR, ("8", "1", "2", "4", "12", "16", "24", "32")), (ENV_SI, ("128", "64", "256")),
          (ENV_FME, ("256", "128", "512"))]
 ENV_ALL = tuple(k for k, _ in KNOBS)

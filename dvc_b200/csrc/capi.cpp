@@ -174,9 +174,13 @@ extern "C" int dvc_ldpca_decode_batch(dvc_ctx *ctx, int count, const int *n, con
   const int n_cif = (int)lists.size();
   for (int i = 0; i < count; i++)
     if (!cw[i].cif) lists.push_back(i);
+  // layout of bt_cw: the codeword descriptors, the two index lists, then (16-byte
+  // aligned, for the 64-bit counter's atomics) the queue heads and the work counter
+  const size_t list_off = sizeof(dvc::LdpcaBatchCw) * count;
+  const size_t ctr_off = (list_off + sizeof(int) * count + 15) & ~(size_t)15;
   if (!c.bt_lr.ensure((size_t)lr_off * 4) || !c.bt_acc.ensure((size_t)byte_off / 8) ||
       !c.bt_dec.ensure((size_t)byte_off) || !c.bt_res.ensure((size_t)count * 16) || !c.bt_ent.ensure((size_t)count * 4) ||
-      !c.bt_cw.ensure(sizeof(dvc::LdpcaBatchCw) * count + sizeof(int) * count + 64) ||
+      !c.bt_cw.ensure(ctr_off + 32) ||
       !c.bt_state.ensure(dvc::ldpca_batch_state_bytes(count))) {
     c.err = "device allocation failed";
     return DVC_E_NOMEM;
@@ -187,15 +191,15 @@ extern "C" int dvc_ldpca_decode_batch(dvc_ctx *ctx, int count, const int *n, con
   A.xt = c.xlm;
   uint8_t *cwb = c.bt_cw.as<uint8_t>();
   A.cw = (const dvc::LdpcaBatchCw *)cwb;
-  int *list_dev = (int *)(cwb + sizeof(dvc::LdpcaBatchCw) * count);
+  int *list_dev = (int *)(cwb + list_off);
   A.cif = list_dev;
   A.qcif = list_dev + n_cif;
   A.n_cif = n_cif;
   A.n_qcif = count - n_cif;
   A.last_cif = Lc->num_codes - 1;
   A.last_qcif = Lq->num_codes - 1;
-  A.ctr = (int *)(list_dev + count);
-  A.work = (unsigned long long *)(A.ctr + 2);
+  A.ctr = (int *)(cwb + ctr_off);
+  A.work = (unsigned long long *)(cwb + ctr_off + 16);
   A.state = c.bt_state.as<dvc::LdpcaBatchState>();
   A.slot_bits = (uint32_t *)(c.bt_state.as<uint8_t>() + sizeof(dvc::LdpcaBatchState) * count);
   A.lr = c.bt_lr.as<float>();

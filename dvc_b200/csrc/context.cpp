@@ -61,10 +61,10 @@ bool Context::init(const char *data, const char *tables, int dev) {
   if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) return false;
   if (!cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate")) return false;
   // process-wide, set by every context creation: CIF 1024 unless the variable
-  // asks for 512, QCIF 256 unless it asks for 512 or 1024
+  // asks for 512, QCIF 1024 unless it asks for 256 or 512
   const char *nt = getenv("DVC_LDPCA_THREADS");
   const char *ntq = getenv("DVC_LDPCA_THREADS_QCIF");
-  set_ldpca_threads(nt ? atoi(nt) : 1024, ntq ? atoi(ntq) : 256);
+  set_ldpca_threads(nt ? atoi(nt) : 1024, ntq ? atoi(ntq) : 1024);
   // the same for the motion searches: threads per updateSI and forward-search block
   const char *si = getenv("DVC_SI_THREADS");
   const char *fme = getenv("DVC_FME_THREADS");

@@ -41,11 +41,12 @@ namespace dvc {
 size_t ldpca_smem_size(int n, int e) { return ldpca_smem_bytes(n, e); }
 
 // One thread block of NT threads per (codeword, speculative slot), each thread
-// holding MAXC = ceil(n / NT) columns.  By default NT = 1024 for CIF codewords
-// (one block per SM: 124 KB of shared memory) and NT = 256 for QCIF ones
-// (31 KB each, four blocks per SM).
-template <int NT, int MAXC>
-__global__ void __launch_bounds__(NT, 1024 / NT)
+// holding MAXC = ceil(n / NT) columns, MINB blocks per SM.  By default NT = 1024 for both lengths
+// (CIF: one block per SM, 124 KB of shared memory; QCIF: 31 KB, 5 edges per
+// thread); QCIF codewords can also run with 256 or 512 threads, four or two
+// blocks per SM (the autotuner measures which is faster).
+template <int NT, int MAXC, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     ldpca_ladder_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, XlmDev xt, int max_iter, int K,
                         LdpcaSpec sp) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT)
   if (J.recons_trans) ld_put_bitplane(g, J, S.dec, n);
 }
 
-template <int NT, int MAXC>
+template <int NT, int MAXC, int MINB>
 static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_jobs, const XlmDev &xt, int max_iter,
                              int K, const LdpcaSpec &sp, cudaStream_t stream) {
   if (L.n > LDPCA_MAX_N || LDPCA_COLS(L.n, NT) > MAXC) return cudaErrorInvalidValue;
@@ -179,40 +180,40 @@ static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_j
   if (e != cudaSuccess) return e;
   const uint64_t bit = 1ull << (dev & 63);
   if (!(attr_set.load() & bit)) {
-    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT, MAXC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT, MAXC, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    // the smallest shared-memory split that holds the blocks an SM can run
-    // (1024 / NT of them), so that the rest of the SM's 256 KB is L1 for the
+    // the smallest shared-memory split that holds the blocks an SM runs (MINB
+    // of them), so that the rest of the SM's 256 KB is L1 for the
     // phi records, which BP iterations re-read (percent of the 228 KB maximum;
     // the driver rounds up to a supported split)
-    const size_t need = (size_t)(1024 / NT) * (smem + 4096);
+    const size_t need = (size_t)MINB * (smem + 4096);
     const int pct = (int)((need * 100 + 228 * 1024 - 1) / (228 * 1024));
-    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT, MAXC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    e = cudaFuncSetAttribute(ldpca_ladder_kernel<NT, MAXC, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              pct > 100 ? 100 : pct);
     if (e != cudaSuccess) return e;
     attr_set.fetch_or(bit);
   }
-  ldpca_ladder_kernel<NT, MAXC><<<num_jobs * K, NT, smem, stream>>>(L, jobs, xt, max_iter, K, sp);
+  ldpca_ladder_kernel<NT, MAXC, MINB><<<num_jobs * K, NT, smem, stream>>>(L, jobs, xt, max_iter, K, sp);
   return cudaGetLastError();
 }
 
-// threads per codeword block: CIF 1024 (or 512), QCIF 256 (or 512, 1024)
-static int g_ldpca_threads = 1024, g_ldpca_threads_qcif = 256;
+// threads per codeword block: CIF 1024 (or 512), QCIF 1024 (or 256, 512)
+static int g_ldpca_threads = 1024, g_ldpca_threads_qcif = 1024;
 
 void set_ldpca_threads(int nt, int nt_qcif) {
   g_ldpca_threads = (nt == 512) ? 512 : 1024;
-  g_ldpca_threads_qcif = (nt_qcif == 512 || nt_qcif == 1024) ? nt_qcif : 256;
+  g_ldpca_threads_qcif = (nt_qcif == 256 || nt_qcif == 512) ? nt_qcif : 1024;
 }
 
 static cudaError_t launch_shape(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
                                 int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream) {
   if (L.n == 1584) {
-    if (g_ldpca_threads_qcif == 1024) return launch_nt<1024, 2>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
-    if (g_ldpca_threads_qcif == 512) return launch_nt<512, 4>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
-    return launch_nt<256, 7>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+    if (g_ldpca_threads_qcif == 1024) return launch_nt<1024, 2, 1>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+    if (g_ldpca_threads_qcif == 512) return launch_nt<512, 4, 2>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+    return launch_nt<256, 7, 4>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
   }
-  if (g_ldpca_threads == 512) return launch_nt<512, 13>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
-  return launch_nt<1024, 7>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+  if (g_ldpca_threads == 512) return launch_nt<512, 13, 1>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
+  return launch_nt<1024, 7, 1>(L, jobs_dev, num_jobs, xt, max_iter, K, sp, stream);
 }
 
 cudaError_t launch_ldpca(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt, int max_iter,

@@ -20,8 +20,8 @@ LdpcaSpec ldpca_spec_carve(void *base, int num_jobs, int K);
 cudaError_t ldpca_spec_reset(const LdpcaSpec &sp, int num_jobs, int K, cudaStream_t stream);
 cudaError_t launch_ldpca_spec(const LadderDev &L, const LdpcaJob *jobs_dev, int num_jobs, const XlmDev &xt,
                               int max_iter, int K, const LdpcaSpec &sp, cudaStream_t stream);
-// threads per codeword block of the ladder kernel: CIF 1024 or 512, QCIF 256,
-// 512 or 1024 (other values select the defaults, 1024 and 256)
+// threads per codeword block of the ladder kernel: CIF 1024 or 512, QCIF 1024,
+// 512 or 256 (other values select the defaults, 1024 for both)
 void set_ldpca_threads(int nt, int nt_qcif);
 // threads per search block of updateSI (64, 128 or 256) and of the forward
 // motion search (128, 256 or 512); other values select 128 and 256

@@ -221,7 +221,7 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
                            const volatile int *bestp, const LdSmem &S, uint32_t *s_ured, int *s_flag, int &iters) {
   constexpr int NT = G::NT;
   constexpr int UNR = 8;                  // edge-pass table reads in flight per thread
-  constexpr int CB = NT >= 1024 ? 1 : 4;  // column-pass columns per batch (3 reads each)
+  constexpr int CB = 1;  // column-pass columns per batch (3 reads each; more spill at 64 registers)
   const int n = L.n, E = L.e, t = g.t, lane = t & 31, warp = t >> 5;
   float *msg = S.msg, *rowt = S.rowt;
   uint8_t *sgd = S.sgd, *rpar = S.rpar, *dec = S.dec;
@@ -272,14 +272,14 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
       rpar[r] = (uint8_t)(syn | (((x & 1u) ^ syn) << 1));
       wrong |= (int)(((x >> 1) ^ syn) & 1u);
     }
-    if (bestp && t == 0) *s_flag = *bestp < code;
+    if (t == 0) *s_flag = bestp ? (int)(*bestp < code) : 0;
     const int any_wrong = g.sync_or(wrong);
     if (it > 0 && !any_wrong) {
       converged = true;
       break;
     }
     // abandon a code above a known success
-    if (it == max_iter || (bestp && *s_flag)) break;
+    if (it == max_iter || *s_flag) break;
     it++;
     // (E) edges: c->v = phi(row sum - own magnitude) with the product of
     //     the other signs

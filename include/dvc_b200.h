@@ -38,7 +38,7 @@ typedef struct dvc_ctx dvc_ctx;
  * dvc_b200.autotune chooses by measurement; decoded output never depends on
  * them): DVC_LDPCA_THREADS = 512 or 1024 threads per CIF codeword block
  * (default 1024) and DVC_LDPCA_THREADS_QCIF = 256, 512 or 1024 per QCIF
- * codeword block (default 256), DVC_SI_THREADS = 64, 128 or 256 threads per
+ * codeword block (default 1024), DVC_SI_THREADS = 64, 128 or 256 threads per
  * updateSI search block (default 128) and DVC_FME_THREADS = 128, 256 or 512
  * per forward-search block (default 256), read here; DVC_LDPCA_SPEC_FLOOR = 1..32, the least number of
  * speculative blocks per codeword in a frame batch (default 8), and
