@@ -292,6 +292,32 @@ class RefStreams:
         return (t if t else r["seconds"]), g - 1
 
 
+def ref_encoder_session(ctx, rs, key, args):
+    """WZ frames/s of the batched session on the reference encoder's streams
+    of the workload (RefStreams): the same timing as `value`."""
+    import torch
+    from dvc_b200 import bitstream as bs
+    streams = {gq: bs.parse_wz(open(wz, "rb").read()) for gq, (wz, ib) in rs.streams.items()}
+    intra_bs = {gq: open(ib, "rb").read() for gq, (wz, ib) in rs.streams.items()}
+    its, lev, src = items(streams, key, intra_starts(streams, intra_bs, key))
+    ses = ctx.session(its, max_batch=args.max_batch, streams=args.streams)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    try:
+        for _ in range(3):
+            ses.run()
+        ms = []
+        for _ in range(max(3, args.steps)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ms.append(ses.run())
+    finally:
+        ses.close()
+    return {"value": len(its) / (float(np.mean(ms)) / 1e3), "unit": "WZ frames/s", "frames": len(its),
+            "ms_per_step": float(np.mean(ms)),
+            "note": "the workload's 16 streams encoded by the reference encoder (its skip and intra decisions), "
+                    "decoded by the batched session as for value"}
+
+
 def ref_plan(n_samples, per_step=4):
     """A fixed stratified sample of the workload: step i decodes one GOP of each
     of `per_step` streams, cycling through all (GOP, QIndex) streams; the GOP
@@ -572,7 +598,7 @@ def main():
     frame_io = len(its) * (11 * fs + fs // 64) + qb * (6336 // 8 + 1)
     frame_io_gbs = frame_io / (step_ms / 1e3) / 1e9
 
-    cpu = None
+    cpu, ref_enc = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             from oracle import refrun
@@ -585,6 +611,9 @@ def main():
                        "sample": "8 GOPs of 8 streams (GOP 2 and 4, QIndex 1-4 and 5-8 in turn) of the same sequence, "
                                  "encoded by the reference encoder, reference DvcDec ParallelMode 1 with every core "
                                  "(decoder-reported decoding time), weighted by the streams' frames"}
+                # the same 640 frames with the reference encoder's mode decisions (the streams the
+                # reference arm decodes), through the same device-resident session
+                ref_enc = ref_encoder_session(ctx, rs, key, args)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "WZ frames/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": "failed: %s" % str(ex)[:200]}
@@ -629,6 +658,7 @@ def main():
                                  "understates the device-wide rate (aggregate_achieved: all launches of a step over "
                                  "the step time)"},
             "cpu_baseline": cpu,
+            "value_reference_encoder_streams": ref_enc,
             "clocks": clk.summary(),
             "gpu_launches": int(prof["kernel_launches"]) * args.steps,
             "graph_replays": ses.replays(),

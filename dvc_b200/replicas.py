@@ -57,3 +57,63 @@ def gather(obj):
     out = [None] * dist.get_world_size()
     dist.all_gather_object(out, obj)
     return out
+
+
+class MultiServer:
+    """Serving across several devices: one server (native.Server, or any object
+    with its submit/poll/finished/result/close methods) per device, and every
+    stream pinned to one of them, so that a stream's frames, which reference
+    each other's decoded output, stay on one device.  A new stream goes to the
+    device with the least load assigned so far (its cost: the caller's
+    estimate, e.g. WZ frames times pixels), ties to the lower device.  Tickets
+    are this object's own and map to (device, that server's ticket).  No data
+    crosses between devices: each decodes its own streams, as a replica."""
+
+    def __init__(self, servers):
+        if not servers:
+            raise ValueError("at least one server")
+        self.servers = list(servers)
+        self.load = [0.0] * len(self.servers)
+        self.device_of = {}   # stream id -> device index
+        self.where = {}       # our ticket -> (device, its ticket)
+        self.back = {}        # (device, its ticket) -> our ticket
+        self.next = 1
+
+    def assign(self, stream, cost=1.0):
+        """The device of `stream`, chosen (least loaded) at its first request."""
+        d = self.device_of.get(stream)
+        if d is None:
+            d = min(range(len(self.servers)), key=lambda i: (self.load[i], i))
+            self.device_of[stream] = d
+            self.load[d] += float(cost)
+        return d
+
+    def submit(self, item, stream, cost=1.0):
+        d = self.assign(stream, cost)
+        t = self.servers[d].submit(item)
+        ours = self.next
+        self.next += 1
+        self.where[ours] = (d, t)
+        self.back[(d, t)] = ours
+        return ours
+
+    def poll(self):
+        """Polls every device; the number of requests that finished."""
+        return sum(int(s.poll() or 0) for s in self.servers)
+
+    def finished(self):
+        out = []
+        for d, s in enumerate(self.servers):
+            out += [self.back[(d, t)] for t in s.finished() if (d, t) in self.back]
+        return sorted(out)
+
+    def result(self, ticket):
+        d, t = self.where.pop(ticket)
+        del self.back[(d, t)]
+        r = self.servers[d].result(t)
+        r["device"] = d
+        return r
+
+    def close(self):
+        for s in self.servers:
+            s.close()

@@ -93,3 +93,37 @@ def test_bench_e2e_form_matches_session(gpu_ctx):
     finally:
         srv.close()
         ses.close()
+
+
+def test_multi_server_replicas_match_alone(gpu_ctx):
+    """Serving over two replicas (dvc_b200.replicas.MultiServer): two contexts,
+    each with its own server, here both on device 0 (this run has one GPU; each
+    replica would take its own device in a multi-GPU deployment, with nothing
+    exchanged between them).  Streams are pinned to a replica; every frame's
+    result equals the frame decoded alone."""
+    from dvc_b200 import replicas
+    streams = [_items("qcif", 5, 2, 4, 41), _items("cif", 3, 2, 3, 42), _items("qcif", 5, 4, 8, 43),
+               _items("cif", 3, 2, 6, 44)]
+    alone = [[gpu_ctx.decode_wz_frames([it])[0] for it in s] for s in streams]
+    ctxs = [native.Context(0), native.Context(0)]
+    ms = replicas.MultiServer([c.server(mem_budget_bytes=4 << 30, streams=2, max_cohort=2) for c in ctxs])
+    try:
+        tickets = {}
+        for s, items in enumerate(streams):
+            for k, it in enumerate(items):
+                tickets[ms.submit(it, stream=s, cost=it["width"] * it["height"] * len(items))] = (s, k)
+        done, t0 = 0, time.time()
+        while done < len(tickets) and time.time() - t0 < 120:
+            done += ms.poll()
+            time.sleep(0.001)
+        assert done == len(tickets)
+        assert sorted(set(ms.device_of.values())) == [0, 1]  # both replicas got streams
+        for t in ms.finished():
+            s, k = tickets[t]
+            r = ms.result(t)
+            assert r["device"] == ms.device_of[s]
+            assert np.array_equal(r["recon"], alone[s][k]["recon"]) and r["wz_bits"] == alone[s][k]["wz_bits"]
+    finally:
+        ms.close()
+        for c in ctxs:
+            c.close()

@@ -73,3 +73,49 @@ def test_two_gloo_ranks_cover_every_stream_once():
     assert sorted(i for s in shares for i in s) == list(range(len(costs)))
     assert [o[1] for o in out] == shares
     assert out[0][3] == out[1][3] == max(o[2] for o in out)
+
+
+class _FakeServer:
+    """A server that finishes every request at the next poll, echoing the item."""
+
+    def __init__(self):
+        self.pending, self.done, self.n = [], {}, 0
+
+    def submit(self, item):
+        self.n += 1
+        self.pending.append((self.n, item))
+        return self.n
+
+    def poll(self):
+        k = len(self.pending)
+        for t, it in self.pending:
+            self.done[t] = {"recon": it["x"], "latency_ms": 1.0}
+        self.pending = []
+        return k
+
+    def finished(self):
+        return sorted(self.done)
+
+    def result(self, t):
+        return self.done.pop(t)
+
+    def close(self):
+        pass
+
+
+def test_multi_server_pins_streams_and_balances_devices():
+    ms = replicas.MultiServer([_FakeServer(), _FakeServer(), _FakeServer()])
+    costs = {0: 5.0, 1: 1.0, 2: 1.0, 3: 4.0, 4: 1.0}
+    tickets = {}
+    for rnd in range(3):
+        for s, c in costs.items():
+            tickets[ms.submit({"x": (s, rnd)}, stream=s, cost=c)] = (s, rnd)
+    # every stream on one device, assigned least-loaded at its first request
+    assert ms.device_of == {0: 0, 1: 1, 2: 2, 3: 1, 4: 2}
+    assert ms.poll() == 15
+    got = {}
+    for t in ms.finished():
+        r = ms.result(t)
+        got[t] = r["recon"]
+        assert r["device"] == ms.device_of[r["recon"][0]]
+    assert got == tickets and ms.finished() == []
