@@ -1,6 +1,6 @@
 """Autotuner for the decoder's launch shapes.
 
-    python -m dvc_b200.autotune [--out tuning.json] [--streams 4] [--frames 33] [--runs 5]
+    python -m dvc_b200.autotune [--out tuning.json] [--streams 4] [--frames 33] [--runs 5] [--bench-workload]
 
 Five launch parameters are chosen by measurement on the device the tuner runs on:
   - threads per CIF codeword block of the LDPCA ladder, 512 or 1024 (edges per
@@ -190,11 +190,22 @@ def main():
     ap.add_argument("--runs", type=int, default=5)
     ap.add_argument("--max-batch", type=int, default=16)
     ap.add_argument("--cuda-streams", type=int, default=16)
+    ap.add_argument("--bench-workload", action="store_true",
+                    help="tune on bench.py's workload (640 CIF WZ frames); the QCIF shape is then not searched")
     args = ap.parse_args()
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     t0 = time.perf_counter()
-    sessions = [workload(args.streams, args.frames, kind="cif"),
-                workload(args.streams * 2, args.frames, seed=4200, kind="qcif")]
+    knobs = KNOBS
+    if args.bench_workload:
+        import sys
+        sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+        import bench
+        ori, key, streams, intra_bs = bench.workload()
+        sessions = [bench.items(streams, key, bench.intra_starts(streams, intra_bs, key))[0]]
+        knobs = [kv for kv in KNOBS if kv[0] != ENV_THREADS_QCIF]
+    else:
+        sessions = [workload(args.streams, args.frames, kind="cif"),
+                    workload(args.streams * 2, args.frames, seed=4200, kind="qcif")]
     print("workload: %s WZ frames (%.1f s to encode)" % ([len(x) for x in sessions], time.perf_counter() - t0),
           flush=True)
     from . import native
@@ -219,7 +230,7 @@ def main():
         print("  %s: median %.1f ms" % (setting, float(np.median(ms_total))), flush=True)
         return ms_total, outputs
 
-    best, results = tune_coordinates(measure)
+    best, results = tune_coordinates(measure, knobs)
     import torch
     device = torch.cuda.get_device_name(dev) if torch.cuda.is_available() else "unknown"
     save(args.out, best, results, device)

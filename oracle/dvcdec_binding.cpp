@@ -4,7 +4,9 @@
 // this repository's GPU library.
 //
 // Built by oracle/Makefile into oracle/_ref/DvcDec_b200: the reference's
-// objects are linked with -Wl,--wrap=decodeGOP, so main's calls of decodeGOP
+// objects (its configuration parser compiled with -DCUDA, as in its GPU build,
+// so that ParallelMode 2 and 3 are accepted: configfile.cpp:278-284) are linked
+// with -Wl,--wrap=decodeGOP, so main's calls of decodeGOP
 // (DvcDec/src/main.cpp:132-142) come here.  With ParallelMode 0 or 1 the call
 // goes on to the reference's own decodeGOP (DVC_Decoder.cpp:26-474).  With
 // ParallelMode 2 or 3 this function does what decodeGOP does around the

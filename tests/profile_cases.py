@@ -2,6 +2,7 @@
 
     python tests/profile_cases.py ldpca-cif     # LDPCA ladder on the CIF golden bitplanes
     python tests/profile_cases.py frame-cif [Q] # one CIF WZ frame (QIndex Q, default 4) through every kernel
+    python tests/profile_cases.py frame-cif-batch [Q] # 16 CIF WZ frames as one batch (one cohort of the bench)
     python tests/profile_cases.py ldpca-micro   # 148 CIF codewords of the LDPCA microbenchmark, one launch
     python tests/profile_cases.py ldpca-batch [N] # N codewords (default 1024) of the batched workload, one launch
 
@@ -34,6 +35,17 @@ def frame_cif(ctx, q=4):
         ctx.decode_wz_frames([it])
 
 
+def frame_cif_batch(ctx, q=4):
+    """16 independent CIF WZ frames (a 33-frame GOP-2 sequence) as one batch:
+    the grids of the batched decode (one cohort of the bench)."""
+    from dvc_b200 import bitstream as bs, decoder, encoder, synth
+    ori, key = synth.make_sequence("cif", 33, 102)
+    st = bs.parse_wz(encoder.encode_sequence(ori, 2, q))
+    its = [decoder.frame_item(st, st.frames[m], key) for (m, b, e) in bs.sequence_order(st.n_frames, st.gop)]
+    for _ in range(2):
+        ctx.decode_wz_frames(its)
+
+
 def ldpca_micro(ctx, count=148):
     from dvc_b200 import ldpca_bench as lb
     lr, acc, crc, x = lb.make_codewords(6336, count, 5)
@@ -51,7 +63,8 @@ def ldpca_batch(ctx, count=1024):
     print("codewords", count, "kernel ms", ms, "bp iterations", work)
 
 
-CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif, "ldpca-micro": ldpca_micro, "ldpca-batch": ldpca_batch}
+CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif, "frame-cif-batch": frame_cif_batch,
+         "ldpca-micro": ldpca_micro, "ldpca-batch": ldpca_batch}
 
 
 def main():
