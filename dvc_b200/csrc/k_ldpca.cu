@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(NT, MINB)
   // the entropy terms (ComputeCE), the bound as a sequential sum in block order
   float llr[MAXC];
   ld_llr(g, n, J.lr, xt, xs, llr, S.msg, (J.llr_out && kk == 0) ? J.llr_out : nullptr);
+  ld_stage_acc(g, J.acc, n, S.accs);
   g.sync();
   if (tid == 0) {
     float h = ld_entropy_sum(S.msg, n);
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(NT, MINB)
       if (s_stop) break;
     }
     int it = 0;
-    const int ok = ld_try_code(g, L, code, llr, J.acc, J.crc, xt, s_pdesc, max_iter, bestp, S, s_ured, &s_stop, it);
+    const int ok = ld_try_code(g, L, code, llr, J.crc, xt, s_pdesc, max_iter, bestp, S, s_ured, &s_stop, it);
     total_iters += it;
     if (ok) {
       if (tid == 0) s_accepted = code;
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(NT, MINB)
   g.sync();
   const int accepted = s_accepted;
   if (accepted == last) {
-    ld_build_syndrome(g, L, last, J.acc, S.rpar);
+    ld_build_syndrome(g, L, last, S.accs, S.rpar);
     g.sync();
     ld_invh_decode(g, L, S.rpar, S.dec, reinterpret_cast<uint32_t *>(S.msg));
   }

@@ -62,7 +62,7 @@ __device__ void finalise(const G &g, const LdpcaBatch &A, const LadderDev &L, in
   LdpcaBatchState &st = A.state[j];
   const int n = L.n, last = L.num_codes - 1, start = st.start;
   if (acc == last) {
-    ld_build_syndrome(g, L, last, A.acc + C.acc_off, S.rpar);
+    ld_build_syndrome(g, L, last, S.accs, S.rpar);
     g.sync();
     ld_invh_decode(g, L, S.rpar, S.dec, reinterpret_cast<uint32_t *>(S.msg));
   } else {
@@ -85,7 +85,7 @@ __device__ void finalise(const G &g, const LdpcaBatch &A, const LadderDev &L, in
       float llr[MAXC];
       ld_llr(g, n, A.lr + C.lr_off, A.xt, xs, llr, nullptr, nullptr);
       int it = 0;
-      ld_try_code(g, L, acc, llr, A.acc + C.acc_off, C.crc, A.xt, pdesc, A.max_iter, nullptr, S, s_ured, s_flag, it);
+      ld_try_code(g, L, acc, llr, C.crc, A.xt, pdesc, A.max_iter, nullptr, S, s_ured, s_flag, it);
     }
     g.sync();
   }
@@ -114,9 +114,10 @@ __device__ void run_item(const G &g, const LdpcaBatch &A, const LadderDev &L, in
   const XlSmall xs = xl_small_global(A.xt);
   float llr[MAXC];
   ld_llr(g, n, A.lr + C.lr_off, A.xt, xs, llr, nullptr, nullptr);
+  ld_stage_acc(g, A.acc + C.acc_off, n, S.accs);
+  g.sync();
   int it = 0;
-  const int ok = ld_try_code(g, L, code, llr, A.acc + C.acc_off, C.crc, A.xt, pdesc, A.max_iter, &st.best, S,
-                             s_ured, s_flag, it);
+  const int ok = ld_try_code(g, L, code, llr, C.crc, A.xt, pdesc, A.max_iter, &st.best, S, s_ured, s_flag, it);
   if (g.t == 0) {
     st.iters[code - start] = it;
     atomicAdd(A.work, (unsigned long long)it);
@@ -269,8 +270,15 @@ size_t ldpca_batch_state_bytes(int count) {
   return (size_t)count * sizeof(LdpcaBatchState) + (size_t)count * kSlots * kWords * 4;
 }
 
+// dynamic shared memory of a batch block: one CIF codeword, or four QCIF ones
+static size_t batch_smem_bytes() {
+  const size_t cif = ldpca_smem_bytes(6336, 3 * 6336), qcif4 = 4 * ldpca_smem_bytes(1584, 3 * 1584);
+  return cif > qcif4 ? cif : qcif4;
+}
+
 cudaError_t launch_ldpca_batch(LdpcaBatch A, int count, int grid, cudaStream_t s) {
-  const size_t smem = ldpca_smem_bytes(LDPCA_MAX_N, 3 * LDPCA_MAX_N);
+  if (A.L_cif.n != 6336 || A.L_qcif.n != 1584) return cudaErrorInvalidValue;
+  const size_t smem = batch_smem_bytes();
   static std::atomic<uint64_t> attr_set{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

@@ -25,13 +25,14 @@
 // packed table (dvc_common.cuh), and the reads of a pass are issued in batches
 // so that several are in flight per thread.
 //
-// Shared memory per codeword (n bits, e edges; CIF n=6336, e=19008: 124 KB;
+// Shared memory per codeword (n bits, e edges; CIF n=6336, e=19008: 125 KB;
 // QCIF a quarter of it):
 //   msg[e]  f32  edge messages by row-order position, in place:
 //                phi(|v->c|) -> c->v -> next phi(|v->c|)
 //   rowt[n] f32  row sums (after decoding: the decoded bits, one byte each)
 //   sgd[e]  u8   bit 0: sign of the v->c message, bit 1: hard decision of its column
 //   rpar[n] u8   bit 0: syndrome bit of the row, bit 1: sign parity of the row
+//   accs[n/8]    the packed accumulated syndrome, staged once per codeword
 #pragma once
 #include <cuda_runtime.h>
 
@@ -52,6 +53,7 @@ __host__ __device__ inline size_t ldpca_smem_bytes(int n, int e) {
   b += (size_t)n * 4;        // rowt
   b += (size_t)e;            // sgd
   b += (size_t)n;            // rpar
+  b += (size_t)n / 8;        // accs
   return (b + 15) & ~(size_t)15;
 }
 
@@ -87,7 +89,7 @@ struct LdGroup {
 
 struct LdSmem {
   float *msg, *rowt;
-  uint8_t *sgd, *rpar, *dec;
+  uint8_t *sgd, *rpar, *dec, *accs;
 };
 
 __device__ __forceinline__ LdSmem ld_carve(uint8_t *base, int n, int e) {
@@ -96,8 +98,18 @@ __device__ __forceinline__ LdSmem ld_carve(uint8_t *base, int n, int e) {
   S.rowt = S.msg + e;
   S.sgd = reinterpret_cast<uint8_t *>(S.rowt + n);
   S.rpar = S.sgd + e;
+  S.accs = S.rpar + n;                          // the codeword's packed accumulated syndrome
   S.dec = reinterpret_cast<uint8_t *>(S.rowt);  // decoded bits, once BP is over
   return S;
+}
+
+// the codeword's packed accumulated syndrome (n/8 bytes, MSB first) into
+// shared memory, one coalesced byte per thread, for every ladder code it tries;
+// the caller synchronises before use
+template <class G>
+__device__ __forceinline__ void ld_stage_acc(const G &g, const uint8_t *packed, int n, uint8_t *accs) {
+  constexpr int NT = G::NT;
+  for (int k = g.t; k < n / 8; k += NT) accs[k] = __ldg(packed + k);
 }
 
 // fused bitplane insertion (putBitplaneToCoeff, bitplane.cpp:4-22)
@@ -137,22 +149,34 @@ __device__ __forceinline__ void ld_invh_decode(const G &g, const LadderDev &L, c
   g.sync();
 }
 
-// one bit of the packed accumulated-syndrome bytes (MSB first, ByteToBit)
+// one bit of the packed accumulated-syndrome bytes (MSB first, ByteToBit),
+// from shared or global memory
 __device__ __forceinline__ uint8_t ld_acc_bit(const uint8_t *packed, int i) {
-  return (uint8_t)((__ldg(packed + (i >> 3)) >> (7 - (i & 7))) & 1);
+  return (uint8_t)((packed[i >> 3] >> (7 - (i & 7))) & 1);
 }
 
-// syndrome of ladder code `code` from the accumulated syndrome (LdpcaDecoder.cpp:684-693)
+// syndrome of ladder code `code` from the accumulated syndrome (LdpcaDecoder.cpp:684-693):
+// bit k of the code is accumulated bit idx[k % nb] + (k / nb) * period xor the
+// same of k - 1.  Thread t takes k = t, t + NT, ...; the quotient and
+// remainder of k by nb advance by those of NT, with no division per bit.
 template <class G>
 __device__ __forceinline__ void ld_build_syndrome(const G &g, const LadderDev &L, int code,
                                                   const uint8_t *packed, uint8_t *synd) {
   constexpr int NT = G::NT;
-  const int m = L.synd_len[code], nb = L.bpp[code];
-  const int *idx = L.idx + (size_t)code * L.period;
+  const int m = L.synd_len[code], nb = L.bpp[code], P = L.period;
+  const int *idx = L.idx + (size_t)code * P;
+  const int dq = NT / nb, dr = NT - dq * nb;
+  int q = g.t / nb, r = g.t - q * nb;
   for (int k = g.t; k < m; k += NT) {
-    uint8_t s = ld_acc_bit(packed, idx[k % nb] + (k / nb) * L.period);
-    if (k > 0) s ^= ld_acc_bit(packed, idx[(k - 1) % nb] + ((k - 1) / nb) * L.period);
+    uint8_t s = ld_acc_bit(packed, __ldg(idx + r) + q * P);
+    if (k > 0) s ^= ld_acc_bit(packed, r > 0 ? __ldg(idx + r - 1) + q * P : __ldg(idx + nb - 1) + (q - 1) * P);
     synd[k] = s;
+    r += dr;
+    q += dq;
+    if (r >= nb) {
+      r -= nb;
+      q++;
+    }
   }
 }
 
@@ -208,7 +232,8 @@ __device__ __forceinline__ int ld_start_code(const LadderDev &L, float h) {
   return start;
 }
 
-// One ladder code below full rate: its syndrome, sum-product BP until every
+// One ladder code below full rate: its syndrome (from the accumulated syndrome
+// staged in S.accs by ld_stage_acc), sum-product BP until every
 // parity check holds (success) or max_iter iterations ran or, when `bestp` is
 // given, a lower code of the same codeword has succeeded (*bestp < code), then
 // the CRC-8 of the hard decision (LdpcaDecoder.cpp:684-693, 718-758).
@@ -217,7 +242,7 @@ __device__ __forceinline__ int ld_start_code(const LadderDev &L, float h) {
 // words of shared memory, s_flag one int, both the group's own.
 template <class G, int MAXC>
 __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int code, const float (&llr)[MAXC],
-                           const uint8_t *acc, int crc, const XlmDev &xt, const uint4 *pdesc, int max_iter,
+                           int crc, const XlmDev &xt, const uint4 *pdesc, int max_iter,
                            const volatile int *bestp, const LdSmem &S, uint32_t *s_ured, int *s_flag, int &iters) {
   constexpr int NT = G::NT;
   constexpr int UNR = 8;                  // edge-pass table reads in flight per thread
@@ -228,7 +253,7 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
   const int m = L.synd_len[code];
   const uint16_t *__restrict__ pos = L.pos + (size_t)code * E;
   const uint16_t *__restrict__ rid = L.rid + (size_t)code * E;
-  ld_build_syndrome(g, L, code, acc, rpar);
+  ld_build_syndrome(g, L, code, S.accs, rpar);
   g.sync();
   const int *rp = L.row_ptr + (size_t)code * (n + 1);
   // first magnitudes: phi(|LLR|) on the three edges of each column
@@ -263,7 +288,24 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
       const int p0 = rp[r], p1 = rp[r + 1];
       float s = 0.0f;
       uint32_t x = 0;  // bit 0: xor of signs, bit 1: xor of decisions
-      for (int p = p0; p < p1; p++) {
+      // low codes have few, long rows (up to ~200 edges): the loads of eight
+      // edges are issued before their adds, which stay in edge order
+      int p = p0;
+      for (; p + 8 <= p1; p += 8) {
+        float v[8];
+        uint32_t b[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          v[q] = msg[p + q];
+          b[q] = sgd[p + q];
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          s += v[q];
+          x ^= b[q];
+        }
+      }
+      for (; p < p1; p++) {
         s += msg[p];
         x ^= sgd[p];
       }
