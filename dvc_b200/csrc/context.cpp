@@ -134,6 +134,27 @@ bool Context::init(const char *data, const char *tables, int dev) {
       return fail("uploading the phi table failed");
     xlm.phi_nbin = (int)(pk.desc.size() / 4);
     phi_bytes = (pk.desc.size() + pk.rec.size() + pk.val.size()) * 4;
+    // optional L2 persisting window over the records of the binades most BP
+    // reads land in (y in [2^-6, 8), exponents 121..129: about 99% of the reads,
+    // 60 MB), so that other kernels' streaming data does not evict them;
+    // DVC_PHI_L2_MB = the set-aside in MB (0 or unset: off)
+    set_phi_window(nullptr, 0, 0.0f);
+    if (const char *mb = getenv("DVC_PHI_L2_MB")) {
+      const size_t want = (size_t)atoi(mb) << 20;
+      const int b_lo = 121 - (int)(xlm.tanh_ylo >> 23), b_hi = 129 - (int)(xlm.tanh_ylo >> 23);
+      if (want > 0 && b_lo >= 0 && b_hi < xlm.phi_nbin) {
+        const size_t r0 = pk.desc[4 * b_lo], r1 = b_hi + 1 < xlm.phi_nbin ? pk.desc[4 * (b_hi + 1)] : pk.rec.size() / 4;
+        int max_persist = 0, max_window = 0;
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, device);
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, device);
+        size_t bytes = (r1 - r0) * 16, aside = want;
+        if (bytes > (size_t)max_window) bytes = (size_t)max_window;
+        if (aside > (size_t)max_persist) aside = (size_t)max_persist;
+        if (bytes > 0 && aside > 0 && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, aside) == cudaSuccess)
+          set_phi_window(xlm.phi_rec + r0, bytes, aside >= bytes ? 1.0f : (float)aside / (float)bytes);
+        cudaGetLastError();
+      }
+    }
   }
 
   if (!near_ties.ensure(8) || !cuda_ok(cudaMemset(near_ties.p, 0, 8), "near-tie counter"))

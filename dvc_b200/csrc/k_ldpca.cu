@@ -169,6 +169,28 @@ __global__ void __launch_bounds__(NT, MINB)
   if (J.recons_trans) ld_put_bitplane(g, J, S.dec, n);
 }
 
+// the L2 persisting window of the table reads (set when a context is created;
+// process-wide like the launch shapes)
+static cudaAccessPolicyWindow g_phi_window = {};
+
+void set_phi_window(const void *base, size_t num_bytes, float hit_ratio) {
+  g_phi_window = cudaAccessPolicyWindow{};
+  if (!base || num_bytes == 0) return;
+  g_phi_window.base_ptr = const_cast<void *>(base);
+  g_phi_window.num_bytes = num_bytes;
+  g_phi_window.hitRatio = hit_ratio;
+  g_phi_window.hitProp = cudaAccessPropertyPersisting;
+  g_phi_window.missProp = cudaAccessPropertyStreaming;
+}
+
+// the window as a launch attribute; returns the number of attributes (0 or 1)
+unsigned phi_window_attr(cudaLaunchAttribute &a) {
+  if (g_phi_window.num_bytes == 0) return 0;
+  a.id = cudaLaunchAttributeAccessPolicyWindow;
+  a.val.accessPolicyWindow = g_phi_window;
+  return 1;
+}
+
 template <int NT, int MAXC, int MINB>
 static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_jobs, const XlmDev &xt, int max_iter,
                              int K, const LdpcaSpec &sp, cudaStream_t stream) {
@@ -194,8 +216,15 @@ static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_j
     if (e != cudaSuccess) return e;
     attr_set.fetch_or(bit);
   }
-  ldpca_ladder_kernel<NT, MAXC, MINB><<<num_jobs * K, NT, smem, stream>>>(L, jobs, xt, max_iter, K, sp);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(num_jobs * K);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  cfg.attrs = attr;
+  cfg.numAttrs = phi_window_attr(attr[0]);
+  return cudaLaunchKernelEx(&cfg, ldpca_ladder_kernel<NT, MAXC, MINB>, L, jobs, xt, max_iter, K, sp);
 }
 
 // threads per codeword block: CIF 1024 (or 512), QCIF 1024 (or 256, 512)

@@ -37,6 +37,8 @@
 
 namespace dvc {
 
+unsigned phi_window_attr(cudaLaunchAttribute &a);
+
 namespace {
 
 constexpr int kSlots = 4;
@@ -297,8 +299,15 @@ cudaError_t launch_ldpca_batch(LdpcaBatch A, int count, int grid, cudaStream_t s
   // the entropy terms (n floats), later the full-rate syndrome, its words and the decoded bits
   ldpca_batch_prep_kernel<<<count, 256, 4 * LDPCA_MAX_N, s>>>(A);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  ldpca_batch_kernel<<<grid, 1024, smem, s>>>(A);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(1024);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  cfg.attrs = attr;
+  cfg.numAttrs = phi_window_attr(attr[0]);
+  return cudaLaunchKernelEx(&cfg, ldpca_batch_kernel, A);
 }
 
 }  // namespace dvc

@@ -26,6 +26,8 @@ void set_ldpca_threads(int nt, int nt_qcif);
 // threads per search block of updateSI (64, 128 or 256) and of the forward
 // motion search (128, 256 or 512); other values select 128 and 256
 void set_me_shapes(int si_threads, int fme_threads);
+// L2 persisting access window of the LDPCA kernels' table reads (num_bytes 0: none)
+void set_phi_window(const void *base, size_t num_bytes, float hit_ratio);
 // batched form: one persistent launch over codewords of both lengths
 // (k_ldpca_batch.cu); state + slot bytes per codeword from ldpca_batch_state_bytes
 size_t ldpca_batch_state_bytes(int count);
