@@ -37,7 +37,7 @@ import numpy as np
 ENV_THREADS, ENV_THREADS_QCIF, ENV_FLOOR = "DVC_LDPCA_THREADS", "DVC_LDPCA_THREADS_QCIF", "DVC_LDPCA_SPEC_FLOOR"
 ENV_SI, ENV_FME = "DVC_SI_THREADS", "DVC_FME_THREADS"
 KNOBS = [(ENV_THREADS, ("1024", "512")), (ENV_THREADS_QCIF, ("1024", "256", "512")),
-         (ENV_FLOOR, ("8", "1", "2", "4", "12", "16", "24", "32")), (ENV_SI, ("128", "64", "256")),
+         (ENV_FLOOR, ("4", "1", "2", "8", "12", "16", "24", "32")), (ENV_SI, ("128", "64", "256")),
          (ENV_FME, ("256", "128", "512"))]
 ENV_ALL = tuple(k for k, _ in KNOBS)
 THREADS = ("1024", "512")

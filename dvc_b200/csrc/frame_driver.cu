@@ -368,12 +368,12 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx.device);
     // speculation pays even on a full GPU (it shortens the slowest codeword of
-    // every lockstep bitplane step, for 7% more BP work at 8 blocks than at 1
-    // on 640 CIF frames, where 8 blocks decode 2x faster than 1 and 3% faster
-    // than 4 or 12); at least 8 blocks per codeword, more when SMs are idle
-    // DVC_LDPCA_SPEC_FLOOR replaces the floor of 8 (the autotuner's setting),
-    // DVC_LDPCA_SPEC fixes the width outright
-    int floor_k = 8;
+    // every lockstep bitplane step); on the bench's 640 CIF frames the
+    // autotuner measured 4 blocks per codeword fastest (911 ms a step, against
+    // 956 at 8, 966 at 2 and 1168 at 1); at least 4 blocks per codeword, more
+    // when SMs are idle.  DVC_LDPCA_SPEC_FLOOR replaces the floor of 4 (the
+    // autotuner's setting), DVC_LDPCA_SPEC fixes the width outright
+    int floor_k = 4;
     if (const char *e = getenv("DVC_LDPCA_SPEC_FLOOR")) floor_k = std::max(1, std::min(32, atoi(e)));
     int k = std::max(floor_k, sms / std::max(1, std::max(nf, concurrent)));
     if (const char *e = getenv("DVC_LDPCA_SPEC")) k = atoi(e);

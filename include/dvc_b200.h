@@ -41,7 +41,7 @@ typedef struct dvc_ctx dvc_ctx;
  * codeword block (default 1024), DVC_SI_THREADS = 64, 128 or 256 threads per
  * updateSI search block (default 128) and DVC_FME_THREADS = 128, 256 or 512
  * per forward-search block (default 256), read here; DVC_LDPCA_SPEC_FLOOR = 1..32, the least number of
- * speculative blocks per codeword in a frame batch (default 8), and
+ * speculative blocks per codeword in a frame batch (default 4), and
  * DVC_LDPCA_SPEC = 1..32, a fixed number instead, both read when a batch is
  * prepared. */
 int dvc_create(const char *data_dir, const char *table_dir, int device, dvc_ctx **out);
