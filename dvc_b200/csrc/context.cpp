@@ -129,11 +129,10 @@ bool Context::init(const char *data, const char *tables, int dev) {
       return true;
     };
     if (!put(pk.desc.data(), pk.desc.size() * 4, (const void **)&xlm.phi_desc) ||
-        !put(pk.rec.data(), pk.rec.size() * 4, (const void **)&xlm.phi_rec) ||
-        !put(pk.val.data(), pk.val.size() * 4, (const void **)&xlm.phi_val))
+        !put(pk.rec.data(), pk.rec.size() * 4, (const void **)&xlm.phi_rec))
       return fail("uploading the phi table failed");
     xlm.phi_nbin = (int)(pk.desc.size() / 4);
-    phi_bytes = (pk.desc.size() + pk.rec.size() + pk.val.size()) * 4;
+    phi_bytes = (pk.desc.size() + pk.rec.size()) * 4;
     // optional L2 persisting window over the records of the binades most BP
     // reads land in (y in [2^-6, 8), exponents 121..129: about 99% of the reads,
     // 60 MB), so that other kernels' streaming data does not evict them;

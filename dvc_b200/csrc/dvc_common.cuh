@@ -90,10 +90,10 @@ __device__ __forceinline__ void xl_phi_stage(const XlmDev &t, uint4 *buf) {
 // least 5e-10 > 2^-31 = tanh_ylo; a smaller one (never formed) clamps to the
 // first entry rather than reading outside the table.  `desc` is the binade
 // descriptor array (staged in shared memory by xl_phi_stage); one 16-byte
-// record read and one 4-byte value read (a rank value, or the first value
-// for delta binades, so that the code has no branch and the reads of several
-// calls can be in flight together).  Both are cached in L1: messages that
-// stay put from one iteration to the next read the same records again.
+// record read per call, the same instructions in every binade, so that the
+// reads of several calls can be in flight together.  Records are cached in
+// L1: messages that stay put from one iteration to the next read the same
+// records again.
 __device__ __forceinline__ float xl_phi(const XlmDev &t, const uint4 *desc, float y) {
   const uint32_t u = __float_as_uint(y);
   const bool one = u >= t.tanh_y1;  // tanhf(y) == 1 (also NaN/negative patterns, never formed)
@@ -102,11 +102,8 @@ __device__ __forceinline__ float xl_phi(const XlmDev &t, const uint4 *desc, floa
   const uint32_t j = i & ((1u << XL_PHI_BINADE_BITS) - 1u);
   const uint32_t g = xl_phi_group(j, d.z);
   const uint4 r = __ldg(t.phi_rec + d.x + g);
-  const uint32_t f = xl_phi_field(j - g * (d.y & 0xffu), d.y, r.y, r.z, r.w);
-  const bool rank = (d.y & XL_PHI_RANK) != 0u;
-  const float rv = __ldg(t.phi_val + (rank ? r.x + f : 0u));
-  const float v = rank ? rv : __uint_as_float(r.x - f);
-  return one ? -0.0f : v;
+  const uint32_t v = xl_phi_decode_bits(j - g * (d.y & 0xffu), d.y, r.x, r.y, r.z, r.w);
+  return one ? -0.0f : __uint_as_float(v);
 }
 
 }  // namespace dvc

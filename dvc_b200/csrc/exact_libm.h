@@ -161,24 +161,26 @@ XL_HD uint32_t xl_tie_dist(double d) {
 // Entry i is the library's phi of the float with bits XL_TANH_YLO + i.  The
 // entries are split into binades (2^23 consecutive patterns, one exponent of
 // y); each binade has a descriptor {first record, format, reciprocal} and is
-// cut into groups of G consecutive entries (4 <= G <= 32), one 16-byte record
-// per group: word 0 the group's base, words 1..3 (96 bits, word 1 lowest) G
-// fields of W = 96 / G bits, field k at bit k*W.  Field k is the offset of
-// entry k from the group's first entry (field 0 is 0):
-//  * delta format: base = bits of the group's first value, field k =
-//    bits(v_0) - bits(v_k) (phi falls as y grows), v_k = base - field k;
-//  * rank format (format bit 16): base = index in the value array of the
-//    group's first value, field k = how many times the value changes from
-//    entry 0 to entry k, v_k = values[base + field k]; used where the values
-//    jump by more than a field holds (large y, where tanhf takes few values)
-//    or where it is smaller.
-// One extract per read, the same for every format, so that lanes reading
-// different binades do not diverge.  The group of binade offset j is
-// j / G = umulhi(j, ceil(2^32 / G)) (exact for j < 2^23, G <= 32).  The
-// builder (libm_tables.cpp) picks the smallest feasible layout per binade and
-// checks every entry of the packed table against the swept one.
+// cut into groups of G consecutive entries, one 16-byte record per group, in
+// one of two formats:
+//  * delta format (4 <= G <= 32): word 0 = bits of the group's first value,
+//    words 1..3 (96 bits, word 1 lowest) G fields of W = 96 / G bits, field k
+//    at bit k*W, field k = bits(v_0) - bits(v_k) (phi falls as y grows; field
+//    0 is 0), v_k = word 0 - field k;
+//  * split format (format bit 16, 2 <= G <= 255): the group holds at most
+//    three distinct values, words 0..2; word 3 holds s1 (bits 0..7) and s2
+//    (bits 8..15): v_k = word 0 for k < s1, word 1 for s1 <= k < s2, word 2
+//    from s2 on.  Used where y >= 2: there tanhf takes few values and phi
+//    jumps by more than a field holds.
+// Either way one 16-byte record read gives the value, and the decode is the
+// same instructions for both formats (both candidates are formed and one is
+// selected), so that lanes reading different binades do not diverge.  The
+// group of binade offset j is j / G = umulhi(j, ceil(2^32 / G)) (exact for
+// j < 2^23, G < 512).  The builder (libm_tables.cpp) picks the smallest
+// feasible layout per binade and checks every entry of the packed table
+// against the swept one.
 #define XL_PHI_BINADE_BITS 23
-#define XL_PHI_RANK 0x10000u
+#define XL_PHI_SPLIT 0x10000u
 #define XL_PHI_MAX_BINADES 64
 
 XL_HD uint32_t xl_umulhi(uint32_t a, uint32_t b) {
@@ -192,7 +194,7 @@ XL_HD uint32_t xl_umulhi(uint32_t a, uint32_t b) {
 // group of binade offset j, recip = ceil(2^32 / G)
 XL_HD uint32_t xl_phi_group(uint32_t j, uint32_t recip) { return xl_umulhi(j, recip); }
 
-// field k of a record's words r1..r3; fmt = G | W << 8 | rank bit
+// field k of a record's words r1..r3; fmt = G | W << 8 (W = 0 in the split format: field 0)
 XL_HD uint32_t xl_phi_field(uint32_t k, uint32_t fmt, uint32_t r1, uint32_t r2, uint32_t r3) {
   const uint32_t w = (fmt >> 8) & 0xffu;
   const uint32_t p = k * w;
@@ -206,9 +208,9 @@ XL_HD uint32_t xl_phi_field(uint32_t k, uint32_t fmt, uint32_t r1, uint32_t r2, 
 #endif
 }
 
-// value of entry k of a group from its record r0..r3 (host form of xl_phi)
-XL_HD float xl_phi_decode(uint32_t k, uint32_t fmt, uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3,
-                          const float *values) {
-  const uint32_t f = xl_phi_field(k, fmt, r1, r2, r3);
-  return (fmt & XL_PHI_RANK) ? values[r0 + f] : xl_bitsf(r0 - f);
+// bits of entry k of a group from its record r0..r3 (both formats; xl_phi reads the record)
+XL_HD uint32_t xl_phi_decode_bits(uint32_t k, uint32_t fmt, uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3) {
+  const uint32_t delta = r0 - xl_phi_field(k, fmt, r1, r2, r3);
+  const uint32_t split = k < (r3 & 0xffu) ? r0 : (k < ((r3 >> 8) & 0xffu) ? r1 : r2);
+  return (fmt & XL_PHI_SPLIT) ? split : delta;
 }

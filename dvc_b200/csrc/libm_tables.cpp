@@ -244,12 +244,12 @@ bool dvc_phi_pack(const float *phi, uint32_t ylo, uint32_t y1, int threads, PhiP
       });
     for (auto &th : ts) th.join();
   };
-  // per binade: the smallest feasible layout.  G entries per record hold
-  // fields of W = 96 / G bits, so a group's span (delta: bits(v_0) - bits of
-  // its last value, which needs the binade to be non-increasing; rank: its
-  // number of changes) must stay below 2^W.  Rank with G = 4 always fits.
+  // per binade: the smallest feasible layout.  Delta: G entries per record
+  // hold fields of W = 96 / G bits, so a group's span (bits(v_0) - bits of its
+  // last value, which needs the binade to be non-increasing) must stay below
+  // 2^W.  Split: every group may change value at most twice; G = 2 always fits.
   std::vector<uint32_t> fmt(nb);
-  std::vector<uint64_t> nrec(nb), nval(nb);
+  std::vector<uint64_t> nrec(nb);
   pool([&](int b) {
     const uint64_t a = (uint64_t)b * B, e = std::min<uint64_t>(n, a + B), len = e - a;
     std::vector<uint32_t> pre(len);  // changes in (a, a + t]
@@ -263,35 +263,30 @@ bool dvc_phi_pack(const float *phi, uint32_t ylo, uint32_t y1, int threads, PhiP
       pre[t] = c;
     }
     uint64_t best = ~0ull;
-    for (uint32_t G = 4; G <= 32; G++) {
+    for (uint32_t G = 2; G <= 255; G++) {
       const uint32_t W = 96 / G;
-      const uint64_t cap = (1ull << W) - 1, recs = (len + G - 1) / G;
+      const uint64_t recs = (len + G - 1) / G;
       uint64_t dmax = 0, rmax = 0;
       for (uint64_t g0 = 0; g0 < len; g0 += G) {
         const uint64_t g1 = std::min<uint64_t>(len, g0 + G) - 1;
         dmax = std::max<uint64_t>(dmax, (uint64_t)bits(a + g0) - bits(a + g1));
         rmax = std::max<uint64_t>(rmax, pre[g1] - pre[g0]);
       }
-      if (mono && dmax <= cap && recs * 16 < best) {
+      if (G >= 4 && G <= 32 && mono && dmax <= ((1ull << W) - 1) && recs * 16 < best) {
         best = recs * 16;
         fmt[b] = G | (W << 8);
         nrec[b] = recs;
-        nval[b] = 0;
       }
-      if (rmax <= cap && recs * 16 + 4ull * (c + 1) < best) {
-        best = recs * 16 + 4ull * (c + 1);
-        fmt[b] = G | (W << 8) | XL_PHI_RANK;
+      if (rmax <= 2 && recs * 16 < best) {
+        best = recs * 16;
+        fmt[b] = G | XL_PHI_SPLIT;
         nrec[b] = recs;
-        nval[b] = c + 1;
       }
     }
   });
-  std::vector<uint64_t> rec0(nb + 1, 0), val0(nb + 1, 0);
-  for (int b = 0; b < nb; b++) {
-    rec0[b + 1] = rec0[b] + nrec[b];
-    val0[b + 1] = val0[b] + nval[b];
-  }
-  if (val0[nb] >= (1ull << 31) || rec0[nb] >= (1ull << 31)) {
+  std::vector<uint64_t> rec0(nb + 1, 0);
+  for (int b = 0; b < nb; b++) rec0[b + 1] = rec0[b] + nrec[b];
+  if (rec0[nb] >= (1ull << 31)) {
     snprintf(err, errlen, "phi table too large to pack");
     return false;
   }
@@ -303,31 +298,33 @@ bool dvc_phi_pack(const float *phi, uint32_t ylo, uint32_t y1, int threads, PhiP
     out.desc[4 * b + 2] = (uint32_t)(((1ull << 32) + G - 1) / G);
   }
   out.rec.assign((size_t)rec0[nb] * 4, 0);
-  // at least one value: delta binades read (and discard) values[0]
-  out.val.assign(std::max<size_t>((size_t)val0[nb], 1), 0.0f);
   pool([&](int b) {
     const uint64_t a = (uint64_t)b * B, e = std::min<uint64_t>(n, a + B);
     const uint32_t G = fmt[b] & 0xffu, W = (fmt[b] >> 8) & 0xffu;
-    const bool rank = (fmt[b] & XL_PHI_RANK) != 0;
+    const bool split = (fmt[b] & XL_PHI_SPLIT) != 0;
     uint32_t *rec = out.rec.data() + rec0[b] * 4;
-    uint64_t v = val0[b];
-    if (rank) out.val[v] = phi[a];
     for (uint64_t g0 = a; g0 < e; g0 += G, rec += 4) {
-      if (rank && g0 > a && bits(g0) != bits(g0 - 1)) out.val[++v] = phi[g0];
-      rec[0] = rank ? (uint32_t)v : bits(g0);
-      uint32_t cnt = 0;
-      for (uint32_t k = 1; k < G && g0 + k < e; k++) {
-        const uint64_t i = g0 + k;
-        uint32_t f;
-        if (rank) {
-          if (bits(i) != bits(i - 1)) {
-            cnt++;
-            out.val[++v] = phi[i];
+      rec[0] = bits(g0);
+      if (split) {
+        // up to three values; s1, s2 = the entries where the second and third start (G: never)
+        uint32_t s1 = G, s2 = G, nv = 1;
+        rec[1] = rec[2] = rec[0];
+        for (uint32_t k = 1; k < G && g0 + k < e; k++) {
+          if (bits(g0 + k) == bits(g0 + k - 1)) continue;
+          if (nv == 1) {
+            s1 = k;
+            rec[1] = rec[2] = bits(g0 + k);
+          } else {
+            s2 = k;
+            rec[2] = bits(g0 + k);
           }
-          f = cnt;
-        } else {
-          f = bits(g0) - bits(i);
+          nv++;
         }
+        rec[3] = s1 | (s2 << 8);
+        continue;
+      }
+      for (uint32_t k = 1; k < G && g0 + k < e; k++) {
+        const uint32_t f = bits(g0) - bits(g0 + k);
         const uint32_t pos = k * W, wi = pos >> 5, sh = pos & 31u;
         rec[1 + wi] |= f << sh;
         if (sh + W > 32) rec[2 + wi] |= f >> (32 - sh);
@@ -341,8 +338,8 @@ bool dvc_phi_pack(const float *phi, uint32_t ylo, uint32_t y1, int threads, PhiP
       const uint32_t *d = out.desc.data() + 4 * (i >> XL_PHI_BINADE_BITS);
       const uint32_t j = (uint32_t)(i & (B - 1)), g = xl_phi_group(j, d[2]);
       const uint32_t *r = out.rec.data() + 4 * ((uint64_t)d[0] + g);
-      const float f = xl_phi_decode(j - g * (d[1] & 0xffu), d[1], r[0], r[1], r[2], r[3], out.val.data());
-      if (xl_fbits(f) != bits(i)) {
+      const uint32_t f = xl_phi_decode_bits(j - g * (d[1] & 0xffu), d[1], r[0], r[1], r[2], r[3]);
+      if (f != bits(i)) {
         if (bad.fetch_add(1) == 0) first_bad = i;
       }
     }
@@ -372,9 +369,11 @@ extern "C" int dvc_phi_table_check(size_t *packed_bytes, char *msg, int msglen) 
     if (msg && msglen > 0) snprintf(msg, (size_t)msglen, "%s", err);
     return -4;  // DVC_E_DATA
   }
-  if (packed_bytes) *packed_bytes = (pk.desc.size() + pk.rec.size() + pk.val.size()) * 4;
+  if (packed_bytes) *packed_bytes = (pk.desc.size() + pk.rec.size()) * 4;
+  size_t nsplit = 0;
+  for (size_t b = 0; b < pk.desc.size() / 4; b++) nsplit += (pk.desc[4 * b + 1] & XL_PHI_SPLIT) != 0;
   if (msg && msglen > 0)
-    snprintf(msg, (size_t)msglen, "%zu entries in %zu binades, %zu records, %zu rank values", phi.size(),
-             pk.desc.size() / 4, pk.rec.size() / 4, pk.val.size());
+    snprintf(msg, (size_t)msglen, "%zu entries in %zu binades, %zu records, %zu split binades", phi.size(),
+             pk.desc.size() / 4, pk.rec.size() / 4, nsplit);
   return 0;
 }

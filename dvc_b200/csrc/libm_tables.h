@@ -34,7 +34,6 @@ typedef struct {
   // -logf(tanhf(y)) for y bits in [tanh_ylo, tanh_y1), packed (exact_libm.h):
   const uint4 *phi_desc;  // per binade: first record, format, ceil(2^32 / G), 0
   const uint4 *phi_rec;   // 16-byte records
-  const float *phi_val;   // values of the rank-format binades (at least one)
   int phi_nbin;           // binades (descriptors), at most XL_PHI_MAX_BINADES
   uint32_t log_mask, exp_mask;  // cap - 1
   int log_shift, exp_shift;     // 32 - log2(cap)
@@ -59,10 +58,9 @@ int dvc_libm_load(const char *path, XlmHost *out, char *err, int errlen);
 void dvc_phi_build(float *out, uint32_t ylo, uint32_t y1, int threads);
 
 // packed form of that table (exact_libm.h): desc holds 4 words per binade,
-// rec 4 words per record, val the rank values
+// rec 4 words per record
 struct PhiPacked {
   std::vector<uint32_t> desc, rec;
-  std::vector<float> val;
 };
 // Packs phi[0 .. y1 - ylo) (ylo must start a binade) and checks every entry
 // of the packed table against phi; returns false with a message on failure.
