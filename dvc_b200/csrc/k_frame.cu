@@ -886,6 +886,13 @@ __global__ void recon_kernel(FrameDev *frames, int band) {
 
 // -------------------------------------------------- side-info refinement
 
+// sum of the four byte differences |a_i - b_i| plus c
+__device__ __forceinline__ uint32_t sad4_acc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
 // updateSI + subPelRefine, sideInfoCreation.cpp:598-736: per WZ block, +-32
 // integer search against the past and future reconstructions (cost = SAD with
 // the motion-vector weight; strict-< row-major argmin), a +-1 half-pel
@@ -941,10 +948,29 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   // can only match or beat the item's best if sad <= floor(best), and only
   // those are weighed; the rest could neither win nor tie.
   const int cw = sr - sl + 1;
-  double bp = 1e300, bf = 1e300;
-  int ip = 0x7fffffff, jf = 0x7fffffff;
   const uint32_t c0 = cur4[0], c1 = cur4[1], c2 = cur4[2], c3 = cur4[3];
-  for (int pc = threadIdx.x; pc < 2 * cw; pc += NT) {
+  // 4x4 SAD of the candidate at window offset (yo, xo) of window wb
+  auto sad_at = [&](const uint8_t *wb, int yo, int xo) {
+    const uint32_t *rw = reinterpret_cast<const uint32_t *>(wb) + ((xo + wo) >> 2) + yo * (WS / 4);
+    const int sh = ((xo + wo) & 3) * 8;
+    uint32_t sad = sad4_acc(__funnelshift_r(rw[0], rw[1], sh), c0, 0u);
+    sad = sad4_acc(__funnelshift_r(rw[WS / 4], rw[WS / 4 + 1], sh), c1, sad);
+    sad = sad4_acc(__funnelshift_r(rw[WS / 2], rw[WS / 2 + 1], sh), c2, sad);
+    return (int)sad4_acc(__funnelshift_r(rw[3 * WS / 4], rw[3 * WS / 4 + 1], sh), c3, sad);
+  };
+  // every thread starts from the zero-motion candidate of each reference (a
+  // candidate like any other, so the lowest (cost, index) is unchanged): its
+  // cost bounds the item's best from the first row on, so a lane weighs only
+  // candidates near the optimum and a warp seldom takes the weighing branch
+  const int y0 = top - st, x0 = left - sl;
+  double bp = (double)sad_at(wp, y0, x0) * d_si_weight[32 * 65 + 32];
+  double bf = (double)sad_at(wf, y0, x0) * d_si_weight[32 * 65 + 32];
+  int ip = y0 * cw + x0, jf = y0 * cw + x0;
+  // whole columns for every thread; the few columns past the last multiple of
+  // NT (2 of the 130 of an interior block at NT = 128) go candidate by
+  // candidate below instead of costing one more pass for a couple of lanes
+  const int ncol = 2 * cw, nstream = ncol > NT ? ncol - ncol % NT : ncol;
+  for (int pc = threadIdx.x; pc < nstream; pc += NT) {
     const bool fut = pc >= cw;
     const int xo = fut ? pc - cw : pc;
     const uint8_t *wb = fut ? wf : wp;
@@ -952,23 +978,24 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     const int sh = ((xo + wo) & 3) * 8;
     const double *wt = d_si_weight + (st - top + 32) * 65 + (sl + xo - left + 32);
     int part[4] = {0, 0, 0, 0};  // running SADs of candidate rows y-3 .. y (indexed by row & 3)
-    double best = 1e300;
-    int bi = 0x7fffffff, thr = 0x7fffffff;
+    double best = fut ? bf : bp;
+    int bi = fut ? jf : ip, thr = (int)best;
     // window row y is row m of candidate y - m; candidate y - 3 is complete at row y
     auto add_row = [&](int y, int slot) {
       const uint32_t *rw = row + y * (WS / 4);
       const uint32_t v = __funnelshift_r(rw[0], rw[1], sh);
-      part[slot & 3] = (int)__vsadu4(v, c0);
-      part[(slot - 1) & 3] += (int)__vsadu4(v, c1);
-      part[(slot - 2) & 3] += (int)__vsadu4(v, c2);
-      part[(slot - 3) & 3] += (int)__vsadu4(v, c3);
+      part[slot & 3] = (int)sad4_acc(v, c0, 0u);
+      part[(slot - 1) & 3] = (int)sad4_acc(v, c1, (uint32_t)part[(slot - 1) & 3]);
+      part[(slot - 2) & 3] = (int)sad4_acc(v, c2, (uint32_t)part[(slot - 2) & 3]);
+      part[(slot - 3) & 3] = (int)sad4_acc(v, c3, (uint32_t)part[(slot - 3) & 3]);
     };
     auto weigh = [&](int yo, int sad) {
       if (sad <= thr) {
         const double cst = (double)sad * __ldg(wt + yo * 65);
-        if (cst < 10000000.0 && cst < best) {  // rows of an item come in increasing index order
+        const int idx = yo * cw + xo;
+        if (cst < 10000000.0 && (cst < best || (cst == best && idx < bi))) {
           best = cst;
-          bi = yo * cw + xo;
+          bi = idx;
           thr = (int)best;
         }
       }
@@ -1009,6 +1036,20 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     }
     if (fut) better(bf, jf, best, bi);
     else better(bp, ip, best, bi);
+  }
+  {
+    const int nrow = wh - 3, nrest = ncol - nstream;
+    for (int k = threadIdx.x; k < nrest * nrow; k += NT) {
+      const int pc = nstream + k / nrow, yo = k - (k / nrow) * nrow;
+      const bool fut = pc >= cw;
+      const int xo = fut ? pc - cw : pc;
+      const int sad = sad_at(fut ? wf : wp, yo, xo);
+      const double cst = (double)sad * __ldg(d_si_weight + (st - top + 32 + yo) * 65 + (sl + xo - left + 32));
+      if (cst < 10000000.0) {
+        if (fut) better(bf, jf, cst, yo * cw + xo);
+        else better(bp, ip, cst, yo * cw + xo);
+      }
+    }
   }
   block_argmin<NT>(bp, ip, scp, sip);
   block_argmin<NT>(bf, jf, scf, sif);
