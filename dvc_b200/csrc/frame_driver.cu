@@ -86,7 +86,7 @@ bool Slot::ensure(int w_, int h_, size_t pdf_floats, size_t in_bytes, size_t out
             mb_mv.ensure(b16n * sizeof(MVd), a) && fmv.ensure(b16n * sizeof(MVd), a) &&
             blk_mv.ensure(b8n * sizeof(MVd), a) && blk_mv2.ensure(b8n * sizeof(MVd), a) && holes.ensure(b16n * 16, a) &&
             mse.ensure(b8n * 8, a) && stats.ensure(32 * 4, a) && in.ensure(in_bytes, a) && out.ensure(out_bytes, a) &&
-            db_img.ensure(fs, a) && db_mode.ensure(2 * n, a) && db_bs.ensure(2 * n * 8, a);
+            db_img.ensure(fs, a) && db_mode.ensure(2 * n, a) && db_bs.ensure(2 * n * 8, a) && si_mv.ensure(2 * n * 4, a);
   w = w_;
   h = h_;
   return ok;
@@ -94,7 +94,8 @@ bool Slot::ensure(int w_, int h_, size_t pdf_floats, size_t in_bytes, size_t out
 
 void Slot::release() {
   DevBuf *all[] = {&si, &dbf, &residue, &side_trans, &recons_trans, &alpha, &lr, &oct, &smf, &pdf,
-                   &mb_mv, &fmv, &blk_mv, &blk_mv2, &holes, &mse, &stats, &in, &out, &db_img, &db_mode, &db_bs};
+                   &mb_mv, &fmv, &blk_mv, &blk_mv2, &holes, &mse, &stats, &in, &out, &db_img, &db_mode, &db_bs,
+                   &si_mv};
   for (DevBuf *b : all) b->release();
 }
 
@@ -292,6 +293,7 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     D.recons_trans = S.recons_trans.as<int>();
     D.alpha = S.alpha.as<float>();
     D.smf = S.smf.as<float>();
+    D.si_mv = S.si_mv.as<int>();
     D.pdf = S.pdf.as<float>();
     D.lr = S.lr.as<float>();
     D.oct = S.oct.as<int16_t>();
@@ -417,6 +419,7 @@ bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileSt
   FrameDev *fdev = frames_dev_.as<FrameDev>();
   for (int f = 0; f < nf; f++) {
     if (!ctx.cuda_ok(cudaMemsetAsync(fd[f].recons_trans, 0, (size_t)w * h * 4, s), "memset")) return false;
+    if (!ctx.cuda_ok(cudaMemsetAsync(fd[f].si_mv, 0xff, (size_t)w * h / 16 * 8, s), "memset")) return false;
     if (!ctx.cuda_ok(cudaMemsetAsync(fd[f].dbf, 0, (size_t)w * h, s), "memset")) return false;
     if (!ctx.cuda_ok(cudaMemsetAsync(fd[f].alpha, 0, (size_t)w * h * 4, s), "memset")) return false;
   }

@@ -52,6 +52,7 @@ struct Slot {
   DevBuf si, dbf, residue, side_trans, recons_trans, alpha, lr, oct, smf, pdf;
   DevBuf mb_mv, fmv, blk_mv, blk_mv2, holes, mse, stats, in, out;
   DevBuf db_img, db_mode, db_bs;  // deblocking: filtered copy, per-edge mode and strength
+  DevBuf si_mv;                   // side-info refinement: last best candidate per WZ block and reference
   bool ensure(int w, int h, size_t pdf_floats, size_t in_bytes, size_t out_bytes, cudaStream_t alloc = nullptr);
   void release();
 };

@@ -23,6 +23,7 @@ struct FrameDev {
   uint8_t *recon, *si, *dbf;
   int *residue, *side_trans, *recons_trans;
   float *alpha, *smf, *pdf, *lr;
+  int *si_mv;                 // [2*nsir] last refinement's best candidate index, past then future (-1: none)
   int16_t *oct;               // [(h-3)*(w-3)*16] over-complete transform of the side information
   MVd *mb_mv, *fmv, *blk_mv, *blk_mv2;
   double *holes, *mse;        // [b16n*2], [b88n]

@@ -958,14 +958,23 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     sad = sad4_acc(__funnelshift_r(rw[WS / 2], rw[WS / 2 + 1], sh), c2, sad);
     return (int)sad4_acc(__funnelshift_r(rw[3 * WS / 4], rw[3 * WS / 4 + 1], sh), c3, sad);
   };
-  // every thread starts from the zero-motion candidate of each reference (a
-  // candidate like any other, so the lowest (cost, index) is unchanged): its
-  // cost bounds the item's best from the first row on, so a lane weighs only
-  // candidates near the optimum and a warp seldom takes the weighing branch
+  // every thread starts from the zero-motion candidate of each reference and
+  // from the best candidate of the block's previous refinement (the window is
+  // the same in every band); they are candidates like any other, so the lowest
+  // (cost, index) is unchanged.  Their cost bounds the item's best from the
+  // first row on, so a lane weighs only candidates near the optimum and a
+  // warp seldom takes the weighing branch
   const int y0 = top - st, x0 = left - sl;
-  double bp = (double)sad_at(wp, y0, x0) * d_si_weight[32 * 65 + 32];
-  double bf = (double)sad_at(wf, y0, x0) * d_si_weight[32 * 65 + 32];
+  auto cost_at = [&](const uint8_t *wb, int idx) {
+    const int yo = idx / cw, xo = idx - (idx / cw) * cw;
+    return (double)sad_at(wb, yo, xo) * d_si_weight[(st - top + 32 + yo) * 65 + (sl + xo - left + 32)];
+  };
+  double bp = cost_at(wp, y0 * cw + x0), bf = cost_at(wf, y0 * cw + x0);
   int ip = y0 * cw + x0, jf = y0 * cw + x0;
+  int *last = F.si_mv + 2 * s_idx;
+  const int lp = last[0], lf = last[1];
+  if (lp >= 0) better(bp, ip, cost_at(wp, lp), lp);
+  if (lf >= 0) better(bf, jf, cost_at(wf, lf), lf);
   // whole columns for every thread; the few columns past the last multiple of
   // NT (2 of the 130 of an interior block at NT = 128) go candidate by
   // candidate below instead of costing one more pass for a couple of lanes
@@ -1053,6 +1062,10 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   }
   block_argmin<NT>(bp, ip, scp, sip);
   block_argmin<NT>(bf, jf, scf, sif);
+  if (threadIdx.x == 0) {
+    last[0] = ip;
+    last[1] = jf;
+  }
   // subPelRefine in the half-pel planes, no vector weight
   // (sideInfoCreation.cpp:598-640): one thread per (reference, offset) SAD,
   // then the strict-< scan over the offsets in the reference's (di, dj) order
