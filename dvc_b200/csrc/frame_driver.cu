@@ -143,9 +143,10 @@ bool FrameBatcher::prepare(Context &ctx, const std::vector<FrameSpec> &frames, c
     if (f.qindex < 1 || f.qindex > 8) return ctx.fail("Qindex out of range 1..8");
     if (!f.past || !f.future || !f.past_ip || !f.future_ip || !f.past_lp || !f.future_lp || !f.recon)
       return ctx.fail("missing device frame pointer");
-    // update_si and the forward motion search read them in 4-byte words
-    if (((uintptr_t)f.past | (uintptr_t)f.future | (uintptr_t)f.past_lp | (uintptr_t)f.future_lp) & 3u)
-      return ctx.fail("reference frames must be 4-byte aligned");
+    // update_si copies the references in 16-byte chunks, the forward motion
+    // search reads the low-pass planes in 4-byte words
+    if ((((uintptr_t)f.past | (uintptr_t)f.future) & 15u) || (((uintptr_t)f.past_lp | (uintptr_t)f.future_lp) & 3u))
+      return ctx.fail("reference frames must be 16-byte aligned (low-pass planes 4-byte)");
     if (!f.crc || !f.acc) return ctx.fail("missing bitplane data");
     if (f.future_idx == f.past_idx) return ctx.fail("past and future reference are the same frame");
   }

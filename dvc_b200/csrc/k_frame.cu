@@ -153,6 +153,42 @@ __device__ __forceinline__ void block_argmin(double &c, int &i, double *sc, int 
   i = si[0];
 }
 
+// block_argmin of two independent (cost, index) pairs in one reduction; sc
+// and si hold 2 * NT / 32 entries
+template <int NT>
+__device__ __forceinline__ void block_argmin2(double &c0, int &i0, double &c1, int &i1, double *sc, int *si) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a0 = __shfl_xor_sync(0xffffffffu, c0, o), a1 = __shfl_xor_sync(0xffffffffu, c1, o);
+    const int j0 = __shfl_xor_sync(0xffffffffu, i0, o), j1 = __shfl_xor_sync(0xffffffffu, i1, o);
+    better(c0, i0, a0, j0);
+    better(c1, i1, a1, j1);
+  }
+  constexpr int NW = NT / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sc[warp] = c0;
+    si[warp] = i0;
+    sc[NW + warp] = c1;
+    si[NW + warp] = i1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < NW; w++) {
+      better(c0, i0, sc[w], si[w]);
+      better(c1, i1, sc[NW + w], si[NW + w]);
+    }
+    sc[0] = c0;
+    si[0] = i0;
+    sc[NW] = c1;
+    si[NW] = i1;
+  }
+  __syncthreads();
+  c0 = sc[0];
+  i0 = si[0];
+  c1 = sc[NW];
+  i1 = si[NW];
+}
+
 // ---------------------------------------------------------------- filters
 
 // lowPassFilter, filter.cpp:214-233
@@ -912,26 +948,30 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   if (sl < 0) sl = 0;
   if (sr > w - 4) sr = w - 4;
   const int ww = sr - sl + 4, wh = sb - st + 4;  // <= 68 x 68
-  // windows with a 72-byte row stride, so that the word after any 4-byte
-  // group of a row is still inside the row
-  constexpr int WS = 72;
+  // windows with a 96-byte row stride: the bytes of [sl & ~15, sl + ww)
+  // (at most 6 16-byte chunks), so that the word after any 4-byte group of a
+  // row is still inside the row
+  constexpr int WS = 96;
   __shared__ __align__(16) uint8_t wp[68 * WS], wf[68 * WS];
   __shared__ uint32_t cur4[4];  // the block's rows, 4 pixels packed per word (first pixel lowest)
   __shared__ int cur[16];
-  __shared__ double scp[NT / 32], scf[NT / 32];
-  __shared__ int sip[NT / 32], sif[NT / 32];
-  // window rows by warp, aligned 4-byte words by lane: the window starts at
-  // byte `wo` of each shared row (w is a multiple of 4, so the words of
-  // [sl & ~3, sl + ww) stay inside the frame row; ww + 3 <= WS)
-  const int wo = sl & 3, nwd = (wo + ww + 3) >> 2;
-  for (int y = threadIdx.x >> 5; y < wh; y += NT / 32) {
-    const uint32_t *pp = reinterpret_cast<const uint32_t *>(F.past + (size_t)(st + y) * w + (sl - wo));
-    const uint32_t *pf = reinterpret_cast<const uint32_t *>(F.future + (size_t)(st + y) * w + (sl - wo));
-    uint32_t *dp = reinterpret_cast<uint32_t *>(wp + y * WS), *df = reinterpret_cast<uint32_t *>(wf + y * WS);
-    for (int x = threadIdx.x & 31; x < nwd; x += 32) {
-      dp[x] = __ldg(pp + x);
-      df[x] = __ldg(pf + x);
+  __shared__ double sca[2 * (NT / 32)];
+  __shared__ int sia[2 * (NT / 32)];
+  // window rows copied in 16-byte chunks straight to shared memory: lanes are
+  // (row of a pair, reference, chunk); w and the planes' bases are multiples
+  // of 16, so the chunks of [sl & ~15, sl + ww) are aligned and stay inside
+  // the frame row; the window starts at byte `wo` of each shared row
+  const int s16 = sl & ~15, wo = sl - s16, nch = (wo + ww + 15) >> 4;
+  {
+    const int lane = threadIdx.x & 31, ch = lane & 7, ref = (lane >> 3) & 1;
+    if (ch < nch) {
+      const uint8_t *src = (ref ? F.future : F.past) + (size_t)st * w + s16 + ch * 16;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared((ref ? wf : wp) + ch * 16);
+      for (int y = 2 * (threadIdx.x >> 5) + (lane >> 4); y < wh; y += 2 * (NT / 32))
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + y * WS), "l"(src + (size_t)y * w)
+                     : "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
   }
   if (threadIdx.x < 16) cur[threadIdx.x] = F.recon[(top + (threadIdx.x >> 2)) * w + left + (threadIdx.x & 3)];
   __syncthreads();
@@ -1060,8 +1100,7 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
       }
     }
   }
-  block_argmin<NT>(bp, ip, scp, sip);
-  block_argmin<NT>(bf, jf, scf, sif);
+  block_argmin2<NT>(bp, ip, bf, jf, sca, sia);
   if (threadIdx.x == 0) {
     last[0] = ip;
     last[1] = jf;
