@@ -754,10 +754,38 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
   if (threadIdx.x == 0) s_dmax += range;
   __syncthreads();
   const int nm = s_n, dmax = s_dmax;
+  const int rmax = 2 * range + 1;
+  if (dmax < NOISE_TAB / 2) {
+    // a symmetric table, etab[ETC + d] = etab[ETC - d] = expf(-a*d), read at
+    // pc - v directly: one address per term, no absolute value
+    constexpr int ETC = NOISE_TAB / 2 - 1;
+    for (int d = threadIdx.x; d <= dmax; d += NT) {
+      const float e = xl_expf(xt, xs, -a * (float)d);
+      etab[ETC + d] = e;
+      etab[ETC - d] = e;
+    }
+    __syncthreads();
+    const int nm4 = (nm + 3) >> 2;
+    const int4 *sc4 = reinterpret_cast<const int4 *>(sc);
+    const float4 *pr4 = reinterpret_cast<const float4 *>(prob);
+    for (int k = threadIdx.x; k < rmax; k += NT) {
+      const float *e0 = etab + ETC + (k - range);
+      float sum = 0.0f;
+      for (int m4 = 0; m4 < nm4; m4++) {
+        const int4 v = sc4[m4];
+        const float4 p = pr4[m4];
+        sum += p.x * e0[-v.x];
+        sum += p.y * e0[-v.y];
+        sum += p.z * e0[-v.z];
+        sum += p.w * e0[-v.w];
+      }
+      out[k] = sum;
+    }
+    return;
+  }
   const int tab = dmax < NOISE_TAB ? dmax + 1 : NOISE_TAB;
   for (int d = threadIdx.x; d < tab; d += NT) etab[d] = xl_expf(xt, xs, -a * (float)d);
   __syncthreads();
-  const int rmax = 2 * range + 1;
   if (dmax < NOISE_TAB) {
     // every distance is in the table: candidates four at a time, in order
     const int nm4 = (nm + 3) >> 2;

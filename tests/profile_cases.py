@@ -5,9 +5,11 @@
     python tests/profile_cases.py frame-cif-batch [Q] # 16 CIF WZ frames as one batch (one cohort of the bench)
     python tests/profile_cases.py ldpca-micro   # 148 CIF codewords of the LDPCA microbenchmark, one launch
     python tests/profile_cases.py ldpca-batch [N] # N codewords (default 1024) of the batched workload, one launch
+    python tests/profile_cases.py bench-step    # one step of bench.py's batched session (640 CIF WZ frames)
 
 Each case runs once after one warm-up run, so a profiler can skip the warm-up
-launches and capture the second instance of a kernel.
+launches and capture the second instance of a kernel; bench-step runs once,
+eagerly (every launch of one step, about 6,100).
 """
 import os
 import sys
@@ -63,11 +65,24 @@ def ldpca_batch(ctx, count=1024):
     print("codewords", count, "kernel ms", ms, "bp iterations", work)
 
 
+def bench_step(ctx):
+    """The batched session of bench.py's workload (16 streams of 16-frame
+    batches), one eager run: the kernels of one timed step."""
+    import bench
+    ori, key, streams, intra_bs = bench.workload()
+    its, lev, src = bench.items(streams, key, bench.intra_starts(streams, intra_bs, key))
+    ses = ctx.session(its, max_batch=16, streams=16)
+    print("step ms", ses.run())
+    ses.close()
+
+
 CASES = {"ldpca-cif": ldpca_cif, "frame-cif": frame_cif, "frame-cif-batch": frame_cif_batch,
-         "ldpca-micro": ldpca_micro, "ldpca-batch": ldpca_batch}
+         "ldpca-micro": ldpca_micro, "ldpca-batch": ldpca_batch, "bench-step": bench_step}
 
 
 def main():
+    # one hardware queue per CUDA stream, as bench.py sets it
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     from dvc_b200 import native
     name = sys.argv[1] if len(sys.argv) > 1 else "ldpca-cif"
     ctx = native.Context(0)
