@@ -1082,11 +1082,21 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     add_row(1, 1);
     add_row(2, 2);
     int y = 3;
-    for (; y + 3 < wh; y += 4) {  // slots of rows y .. y+3 are 3, 0, 1, 2 (y = 3 mod 4)
+    // slots of rows y .. y+3 are 3, 0, 1, 2 (y = 3 mod 4); the four candidates
+    // completed by a group are weighed after it, in order, and only when one
+    // lane of the warp has one that can match its best (the lanes run the same
+    // rows, so the vote is taken by the whole active warp): a warp branches
+    // once per four rows, and rarely
+    for (; y + 3 < wh; y += 4) {
+      int sd[4];
 #pragma unroll
       for (int r = 0; r < 4; r++) {
         add_row(y + r, 3 + r);
-        weigh(y + r - 3, part[(3 + r - 3) & 3]);
+        sd[r] = part[r & 3];
+      }
+      if (__any_sync(__activemask(), min(min(sd[0], sd[1]), min(sd[2], sd[3])) <= thr)) {
+#pragma unroll
+        for (int r = 0; r < 4; r++) weigh(y + r - 3, sd[r]);
       }
     }
     for (; y < wh; y++) {  // the last rows; y - 3 mod 4 as above
