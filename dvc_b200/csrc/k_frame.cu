@@ -153,16 +153,26 @@ __device__ __forceinline__ void block_argmin(double &c, int &i, double *sc, int 
   i = si[0];
 }
 
-// block_argmin of two independent (cost, index) pairs in one reduction; sc
-// and si hold 2 * NT / 32 entries
+// lowest (cost, index) over a full warp for costs >= 0 (never NaN): a
+// non-negative double orders like its bit pattern, so three 32-bit warp
+// reductions give it (high word, low word among the lanes that hold the
+// smallest high word, index among the lanes that hold the smallest cost)
+__device__ __forceinline__ void warp_argmin_nonneg(double &c, int &i) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(c);
+  const unsigned hw = (unsigned)(b >> 32), lw = (unsigned)b;
+  const unsigned mh = __reduce_min_sync(0xffffffffu, hw);
+  const unsigned ml = __reduce_min_sync(0xffffffffu, hw == mh ? lw : 0xffffffffu);
+  const unsigned mi = __reduce_min_sync(0xffffffffu, (hw == mh && lw == ml) ? (unsigned)i : 0xffffffffu);
+  c = __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+  i = (int)mi;
+}
+
+// block_argmin of two independent (cost, index) pairs with costs >= 0 in one
+// reduction; sc and si hold 2 * NT / 32 entries
 template <int NT>
 __device__ __forceinline__ void block_argmin2(double &c0, int &i0, double &c1, int &i1, double *sc, int *si) {
-  for (int o = 16; o > 0; o >>= 1) {
-    const double a0 = __shfl_xor_sync(0xffffffffu, c0, o), a1 = __shfl_xor_sync(0xffffffffu, c1, o);
-    const int j0 = __shfl_xor_sync(0xffffffffu, i0, o), j1 = __shfl_xor_sync(0xffffffffu, i1, o);
-    better(c0, i0, a0, j0);
-    better(c1, i1, a1, j1);
-  }
+  warp_argmin_nonneg(c0, i0);
+  warp_argmin_nonneg(c1, i1);
   constexpr int NW = NT / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
@@ -1032,21 +1042,34 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
   // (cost, index) is unchanged.  Their cost bounds the item's best from the
   // first row on, so a lane weighs only candidates near the optimum and a
   // warp seldom takes the weighing branch
+  // (lanes 0-3 of each warp weigh the four starts; the warp shares them)
   const int y0 = top - st, x0 = left - sl;
-  auto cost_at = [&](const uint8_t *wb, int idx) {
-    const int yo = idx / cw, xo = idx - (idx / cw) * cw;
-    return (double)sad_at(wb, yo, xo) * d_si_weight[(st - top + 32 + yo) * 65 + (sl + xo - left + 32)];
-  };
-  double bp = cost_at(wp, y0 * cw + x0), bf = cost_at(wf, y0 * cw + x0);
-  int ip = y0 * cw + x0, jf = y0 * cw + x0;
   int *last = F.si_mv + 2 * s_idx;
-  const int lp = last[0], lf = last[1];
-  if (lp >= 0) better(bp, ip, cost_at(wp, lp), lp);
-  if (lf >= 0) better(bf, jf, cost_at(wf, lf), lf);
-  // whole columns for every thread; the few columns past the last multiple of
-  // NT (2 of the 130 of an interior block at NT = 128) go candidate by
-  // candidate below instead of costing one more pass for a couple of lanes
-  const int ncol = 2 * cw, nstream = ncol > NT ? ncol - ncol % NT : ncol;
+  double bp, bf;
+  int ip, jf;
+  {
+    const int lane = threadIdx.x & 31;
+    // lane 0: zero motion in the past window, 1: in the future one, 2 and 3:
+    // the previous band's best in each (-1 before the first band)
+    const int idx = lane < 2 ? y0 * cw + x0 : (lane < 4 ? last[lane - 2] : -1);
+    double c = 1e300;
+    if (idx >= 0) {
+      const int yo = idx / cw, xo = idx - yo * cw;
+      c = (double)sad_at((lane & 1) ? wf : wp, yo, xo) * d_si_weight[(st - top + 32 + yo) * 65 + (sl + xo - left + 32)];
+    }
+    bp = __shfl_sync(0xffffffffu, c, 0);
+    bf = __shfl_sync(0xffffffffu, c, 1);
+    ip = jf = y0 * cw + x0;
+    const double c2 = __shfl_sync(0xffffffffu, c, 2), c3 = __shfl_sync(0xffffffffu, c, 3);
+    const int i2 = __shfl_sync(0xffffffffu, idx, 2), i3 = __shfl_sync(0xffffffffu, idx, 3);
+    if (i2 >= 0) better(bp, ip, c2, i2);
+    if (i3 >= 0) better(bf, jf, c3, i3);
+  }
+  // whole columns for every thread; when at most two columns are past the
+  // last multiple of NT (2 of the 130 of an interior block at NT = 64 or
+  // 128) they go candidate by candidate below instead of costing one more
+  // pass for a couple of lanes
+  const int ncol = 2 * cw, nstream = (ncol > NT && ncol % NT <= 2) ? ncol - ncol % NT : ncol;
   for (int pc = threadIdx.x; pc < nstream; pc += NT) {
     const bool fut = pc >= cw;
     const int xo = fut ? pc - cw : pc;
@@ -1125,9 +1148,10 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     else better(bp, ip, best, bi);
   }
   {
+    // at most two columns remain: the column of candidate k is k >= nrow
     const int nrow = wh - 3, nrest = ncol - nstream;
     for (int k = threadIdx.x; k < nrest * nrow; k += NT) {
-      const int pc = nstream + k / nrow, yo = k - (k / nrow) * nrow;
+      const int hi = k >= nrow, pc = nstream + hi, yo = k - hi * nrow;
       const bool fut = pc >= cw;
       const int xo = fut ? pc - cw : pc;
       const int sad = sad_at(fut ? wf : wp, yo, xo);
