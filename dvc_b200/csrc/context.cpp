@@ -132,6 +132,21 @@ bool Context::init(const char *data, const char *tables, int dev) {
         !put(pk.rec.data(), pk.rec.size() * 4, (const void **)&xlm.phi_rec))
       return fail("uploading the phi table failed");
     xlm.phi_nbin = (int)(pk.desc.size() / 4);
+    {
+      int max_linear = 0;
+      cudaDeviceGetAttribute(&max_linear, cudaDevAttrMaxTexture1DLinearWidth, device);
+      if ((size_t)max_linear < pk.rec.size() / 4) return fail("phi table exceeds the linear texture limit");
+      cudaResourceDesc rd = {};
+      rd.resType = cudaResourceTypeLinear;
+      rd.res.linear.devPtr = const_cast<uint4 *>(xlm.phi_rec);
+      rd.res.linear.desc = cudaCreateChannelDesc<uint4>();
+      rd.res.linear.sizeInBytes = pk.rec.size() * 4;
+      cudaTextureDesc td = {};
+      td.readMode = cudaReadModeElementType;
+      cudaTextureObject_t tex = 0;
+      if (cudaCreateTextureObject(&tex, &rd, &td, nullptr) != cudaSuccess) return fail("phi texture object");
+      xlm.phi_tex = tex;
+    }
     phi_bytes = (pk.desc.size() + pk.rec.size()) * 4;
     // optional L2 persisting window over the records of the binades most BP
     // reads land in (y in [2^-6, 8), exponents 121..129: about 99% of the reads,
@@ -176,6 +191,8 @@ bool Context::init(const char *data, const char *tables, int dev) {
 void Context::release() {
   for (auto &g : ladders_gpu) g.release();
   ladders_gpu.clear();
+  if (xlm.phi_tex) cudaDestroyTextureObject((cudaTextureObject_t)xlm.phi_tex);
+  xlm.phi_tex = 0;
   for (void *p : xlm_allocs) cudaFree(p);
   xlm_allocs.clear();
   ld_lr.release();

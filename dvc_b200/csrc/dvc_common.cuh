@@ -101,7 +101,7 @@ __device__ __forceinline__ float xl_phi(const XlmDev &t, const uint4 *desc, floa
   const uint4 d = desc[i >> XL_PHI_BINADE_BITS];
   const uint32_t j = i & ((1u << XL_PHI_BINADE_BITS) - 1u);
   const uint32_t g = xl_phi_group(j, d.z);
-  const uint4 r = __ldg(t.phi_rec + d.x + g);
+  const uint4 r = tex1Dfetch<uint4>((cudaTextureObject_t)t.phi_tex, (int)(d.x + g));
   const uint32_t v = xl_phi_decode_bits(j - g * (d.y & 0xffu), d.y, r.x, r.y, r.z, r.w);
   return one ? -0.0f : __uint_as_float(v);
 }

@@ -40,6 +40,10 @@ typedef struct {
   uint32_t tanh_ylo, tanh_y1;
   uint32_t exp_tie;
   const XlmSmallTables *small;  // device copy
+  // phi_rec as a texture object (cudaTextureObject_t; element reads, no
+  // filtering): the BP kernels gather the records through the texture path,
+  // which leaves the load/store path to their shared-memory traffic
+  unsigned long long phi_tex;
 } XlmDev;
 
 #ifdef __cplusplus
