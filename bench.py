@@ -651,10 +651,10 @@ def main():
                                               "planes, output, syndromes and CRCs, mode map) at the batched rate: "
                                               "the path is bound by its gathers and compute, not by moving "
                                               "these bytes"},
-                         "note": "4-byte phi values gathered at random, one 16-byte record each, from a packed "
-                                 "166 MB table whose hot part mostly stays in L2 (82% L2 hits, ~152 KB of DRAM "
-                                 "traffic per block-iteration in ncu); the kernel is bound by the latency of those "
-                                 "gathers and by L1TEX throughput, not by DRAM bandwidth.  Launches of 16 streams "
+                         "note": "4-byte phi values gathered at random, one 16-byte record each through the "
+                                 "texture path, from a packed 166 MB table whose hot part mostly stays in L2 (84% "
+                                 "L2 hits, ~125 KB of DRAM traffic per block-iteration in ncu); the kernel is bound "
+                                 "by the latency of those gathers, not by DRAM bandwidth.  Launches of 16 streams "
                                  "overlap, so the per-launch figure understates the device-wide rate "
                                  "(aggregate_achieved: all launches of a step over the step time)"},
             "cpu_baseline": cpu,
