@@ -45,6 +45,13 @@ size_t ldpca_smem_size(int n, int e) { return ldpca_smem_bytes(n, e); }
 // (CIF: one block per SM, 124 KB of shared memory; QCIF: 31 KB, 5 edges per
 // thread); QCIF codewords can also run with 256 or 512 threads, four or two
 // blocks per SM (the autotuner measures which is faster).
+// the QCIF shape that owns its SM stages the code's index tables in shared
+// memory (ld_try_code); the others read them from global memory
+template <int NT, int MAXC>
+__host__ __device__ constexpr bool ldpca_stage() {
+  return NT == 1024 && MAXC <= 2;
+}
+
 template <int NT, int MAXC, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     ldpca_ladder_kernel(LadderDev L, const LdpcaJob *__restrict__ jobs, XlmDev xt, int max_iter, int K,
@@ -56,7 +63,7 @@ __global__ void __launch_bounds__(NT, MINB)
   const bool spec = sp.best != nullptr;
   const LdGroup<NT, true> g{(int)threadIdx.x, 0};
   const int n = L.n, tid = threadIdx.x;
-  const LdSmem S = ld_carve(smem, n, L.e);
+  const LdSmem S = ld_carve(smem, n, L.e, ldpca_stage<NT, MAXC>());
   __shared__ uint32_t s_ured[NT / 32];
   __shared__ int s_start, s_accepted, s_stop;
   __shared__ uint4 s_pdesc[XL_PHI_MAX_BINADES];
@@ -93,7 +100,8 @@ __global__ void __launch_bounds__(NT, MINB)
       if (s_stop) break;
     }
     int it = 0;
-    const int ok = ld_try_code(g, L, code, llr, J.crc, xt, s_pdesc, max_iter, bestp, S, s_ured, &s_stop, it);
+    const int ok = ld_try_code<LdGroup<NT, true>, MAXC, ldpca_stage<NT, MAXC>()>(g, L, code, llr, J.crc, xt, s_pdesc,
+                                                                                  max_iter, bestp, S, s_ured, &s_stop, it);
     total_iters += it;
     if (ok) {
       if (tid == 0) s_accepted = code;
@@ -195,7 +203,7 @@ template <int NT, int MAXC, int MINB>
 static cudaError_t launch_nt(const LadderDev &L, const LdpcaJob *jobs, int num_jobs, const XlmDev &xt, int max_iter,
                              int K, const LdpcaSpec &sp, cudaStream_t stream) {
   if (L.n > LDPCA_MAX_N || LDPCA_COLS(L.n, NT) > MAXC) return cudaErrorInvalidValue;
-  const size_t smem = ldpca_smem_bytes(L.n, L.e);
+  const size_t smem = ldpca_smem_bytes(L.n, L.e, ldpca_stage<NT, MAXC>());
   // the attributes are per device: set them once for each device
   static std::atomic<uint64_t> attr_set{0};
   int dev = 0;

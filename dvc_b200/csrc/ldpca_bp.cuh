@@ -48,9 +48,12 @@ namespace dvc {
 // columns per thread of a group of nt threads on codewords of n bits
 #define LDPCA_COLS(n, nt) (((n) + (nt) - 1) / (nt))
 
-__host__ __device__ inline size_t ldpca_smem_bytes(int n, int e) {
-  size_t b = (size_t)e * 4;  // msg
-  b += (size_t)n * 4;        // rowt
+// stage: the ladder code's index tables (rid, pos: 2 x e uint16) live in
+// shared memory too (see ld_try_code)
+__host__ __device__ inline size_t ldpca_smem_bytes(int n, int e, bool stage = false) {
+  size_t b = (size_t)e * 4;       // msg
+  if (stage) b += (size_t)e * 4;  // rid and pos of the code tried
+  b += (size_t)n * 4;             // rowt
   b += (size_t)e;            // sgd
   b += (size_t)n;            // rpar
   b += (size_t)n / 8;        // accs
@@ -89,13 +92,16 @@ struct LdGroup {
 
 struct LdSmem {
   float *msg, *rowt;
+  uint16_t *rid, *pos;  // staged index tables of the code tried (null: read from global memory)
   uint8_t *sgd, *rpar, *dec, *accs;
 };
 
-__device__ __forceinline__ LdSmem ld_carve(uint8_t *base, int n, int e) {
+__device__ __forceinline__ LdSmem ld_carve(uint8_t *base, int n, int e, bool stage = false) {
   LdSmem S;
   S.msg = reinterpret_cast<float *>(base);
-  S.rowt = S.msg + e;
+  S.rid = stage ? reinterpret_cast<uint16_t *>(S.msg + e) : nullptr;  // e is a multiple of 8: 16-byte aligned
+  S.pos = stage ? S.rid + e : nullptr;
+  S.rowt = stage ? reinterpret_cast<float *>(S.pos + e) : S.msg + e;
   S.sgd = reinterpret_cast<uint8_t *>(S.rowt + n);
   S.rpar = S.sgd + e;
   S.accs = S.rpar + n;                          // the codeword's packed accumulated syndrome
@@ -240,7 +246,14 @@ __device__ __forceinline__ int ld_start_code(const LadderDev &L, float h) {
 // Returns 1 when the code decodes with a matching CRC; the decoded bits are
 // then in S.dec.  `iters` receives the BP iterations run.  s_ured holds NT/32
 // words of shared memory, s_flag one int, both the group's own.
-template <class G, int MAXC>
+// an index table entry: a shared-memory read when staged, a read-only global one otherwise
+template <bool STAGE>
+__device__ __forceinline__ int ld_idx(const uint16_t *p) {
+  if constexpr (STAGE) return *p;
+  else return __ldg(p);
+}
+
+template <class G, int MAXC, bool STAGE = false>
 __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int code, const float (&llr)[MAXC],
                            int crc, const XlmDev &xt, const uint4 *pdesc, int max_iter,
                            const volatile int *bestp, const LdSmem &S, uint32_t *s_ured, int *s_flag, int &iters) {
@@ -251,8 +264,24 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
   float *msg = S.msg, *rowt = S.rowt;
   uint8_t *sgd = S.sgd, *rpar = S.rpar, *dec = S.dec;
   const int m = L.synd_len[code];
+  // STAGE: the code's index tables are copied to shared memory for the whole
+  // try (e is a multiple of 8: 16-byte copies), which keeps a global round
+  // trip off the chain leading to every table gather.  Only where the block
+  // owns its SM and the copy leaves the shared-memory carveout (so the L1
+  // that the in-flight table gathers allocate in) unchanged: QCIF codewords
+  // on 1024 threads.  At CIF the 76 KB of tables would cut L1 to a fifth.
   const uint16_t *__restrict__ pos = L.pos + (size_t)code * E;
   const uint16_t *__restrict__ rid = L.rid + (size_t)code * E;
+  if constexpr (STAGE) {
+    const uint4 *gr = reinterpret_cast<const uint4 *>(rid), *gp = reinterpret_cast<const uint4 *>(pos);
+    uint4 *sr = reinterpret_cast<uint4 *>(S.rid), *sp = reinterpret_cast<uint4 *>(S.pos);
+    for (int i = t; i < E / 8; i += NT) {
+      sr[i] = __ldg(gr + i);
+      sp[i] = __ldg(gp + i);
+    }
+    pos = S.pos;
+    rid = S.rid;
+  }
   ld_build_syndrome(g, L, code, S.accs, rpar);
   g.sync();
   const int *rp = L.row_ptr + (size_t)code * (n + 1);
@@ -269,7 +298,7 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
         const uint8_t ng = (uint8_t)(__float_as_uint(llr[c]) >> 31);
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-          const int p = __ldg(pos + 3 * k + i);
+          const int p = ld_idx<STAGE>(pos + 3 * k + i);
           msg[p] = ph[c];
           sgd[p] = ng;
         }
@@ -333,7 +362,7 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
         // lanes past the last edge repeat it (no branch, so that the UNR
         // table reads are in flight together) and store nothing
         const int p = min(p0 + q * NT, E - 1);
-        rr[q] = __ldg(rid + p);
+        rr[q] = ld_idx<STAGE>(rid + p);
         c[q] = xl_phi(xt, pdesc, (rowt[rr[q]] - msg[p] + 1e-9f) / 2.0f);
       }
 #pragma unroll
@@ -357,7 +386,7 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
           float mv[3];
 #pragma unroll
           for (int i = 0; i < 3; i++) {
-            pp[b][i] = __ldg(pos + 3 * k + i);
+            pp[b][i] = ld_idx<STAGE>(pos + 3 * k + i);
             mv[i] = msg[pp[b][i]];
           }
           float tmp = llr[c];
@@ -396,7 +425,7 @@ __device__ __forceinline__ int ld_try_code(const G &g, const LadderDev &L, int c
   // linear for a fixed length with zero initial value and no final xor)
   uint32_t cr = 0;
   for (int k = t; k < n; k += NT) {
-    const uint8_t d = (uint8_t)((sgd[__ldg(pos + 3 * k)] >> 1) & 1u);
+    const uint8_t d = (uint8_t)((sgd[ld_idx<STAGE>(pos + 3 * k)] >> 1) & 1u);
     dec[k] = d;
     if (d) cr ^= __ldg(L.crc_tab + k);
   }
