@@ -53,7 +53,8 @@ int qbits_per_block(int q) {
 cudaError_t upload_transform_scales(const double *post, const double *pre);
 cudaError_t launch_side_info(FrameDev *fr, int nf, int w, int h, cudaStream_t s);
 cudaError_t launch_frame_prep(FrameDev *fr, int nf, int w, int h, cudaStream_t s);
-cudaError_t launch_noise_dist(FrameDev *fr, int nf, int max_nsir, const XlmDev &xt, int band, cudaStream_t s);
+cudaError_t launch_noise_dist(FrameDev *fr, int nf, int max_nsir, const XlmDev &xt, int band, int max_range,
+                              cudaStream_t s);
 cudaError_t launch_cond_bit(FrameDev *fr, int nf, int w, int h, int band, int bit, cudaStream_t s);
 cudaError_t launch_band_end(FrameDev *fr, int nf, int w, int h, int max_nsir, int band, const XlmDev &xt,
                             cudaStream_t s);
@@ -447,7 +448,10 @@ bool FrameBatcher::execute(Context &ctx, cudaStream_t s, int max_iter, ProfileSt
   size_t si = 0;
   while (si < steps.size()) {
     const int band = steps[si].band;
-    if (!ctx.cuda_ok(launch_noise_dist(fdev, nf, max_nsir, ctx.xlm, band, s), "noise distribution")) return false;
+    int max_range = 0;
+    for (int f = 0; f < nf; f++) max_range = std::max(max_range, fd[f].crange[kZigzag[band]]);
+    if (!ctx.cuda_ok(launch_noise_dist(fdev, nf, max_nsir, ctx.xlm, band, max_range, s), "noise distribution"))
+      return false;
     for (; si < steps.size() && steps[si].band == band; si++) {
       if (!ctx.cuda_ok(launch_cond_bit(fdev, nf, w, h, band, steps[si].bit, s), "conditional bit probability"))
         return false;

@@ -712,7 +712,35 @@ __device__ __forceinline__ Win ml_window(int top, int left, int w, int h) {
 // depends only on the integer distance d = |k - range - s_m|, so each block
 // first tabulates expf(-alpha*d) (the same float expression) for every d it
 // needs, then sums the 81-candidate mixture in the reference's order.
-#define NOISE_TAB 4096
+#define NOISE_TAB 2048
+
+// The mixture for up to four values of one lane, k0 + c * 32 * NW (c < NC):
+// one table address per candidate serves all of them through immediate
+// offsets.  Each value's sum still runs over the candidates in order.
+template <int NC, int NW>
+__device__ __forceinline__ void noise_mix(const float *e0, const int4 *sc4, const float4 *pr4, int nm4, float *out,
+                                          int k0, int rmax) {
+  float s[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) s[c] = 0.0f;
+  for (int m4 = 0; m4 < nm4; m4++) {
+    const int4 v = sc4[m4];
+    const float4 p = pr4[m4];
+    const float *ax = e0 - v.x, *ay = e0 - v.y, *az = e0 - v.z, *aw = e0 - v.w;
+#pragma unroll
+    for (int c = 0; c < NC; c++) s[c] += p.x * ax[c * 32 * NW];
+#pragma unroll
+    for (int c = 0; c < NC; c++) s[c] += p.y * ay[c * 32 * NW];
+#pragma unroll
+    for (int c = 0; c < NC; c++) s[c] += p.z * az[c * 32 * NW];
+#pragma unroll
+    for (int c = 0; c < NC; c++) s[c] += p.w * aw[c * 32 * NW];
+  }
+#pragma unroll
+  for (int c = 0; c < NC; c++)
+    if (k0 + c * 32 * NW < rmax) out[k0 + c * 32 * NW] = s[c];
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev xt, int band) {
   FrameDev &F = frames[blockIdx.y];
@@ -765,31 +793,40 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
   __syncthreads();
   const int nm = s_n, dmax = s_dmax;
   const int rmax = 2 * range + 1;
-  if (dmax < NOISE_TAB / 2) {
+  if (dmax < NOISE_TAB / 2 - 32) {
     // a symmetric table, etab[ETC + d] = etab[ETC - d] = expf(-a*d), read at
-    // pc - v directly: one address per term, no absolute value
+    // pc - v directly: one address per term, no absolute value.  Values are
+    // taken in groups of 32 (one per lane); warp w takes groups w, w + NW, ...,
+    // up to four per pass.  The last group of a block reads up to 31 entries
+    // past dmax for values past rmax, which are not stored: those entries
+    // hold 0.
     constexpr int ETC = NOISE_TAB / 2 - 1;
-    for (int d = threadIdx.x; d <= dmax; d += NT) {
-      const float e = xl_expf(xt, xs, -a * (float)d);
-      etab[ETC + d] = e;
-      etab[ETC - d] = e;
+    constexpr int NW = NT / 32;
+    for (int d = threadIdx.x; d <= dmax + 31; d += NT) {
+      if (d <= dmax) {
+        const float e = xl_expf(xt, xs, -a * (float)d);
+        etab[ETC + d] = e;
+        etab[ETC - d] = e;
+      } else {
+        etab[ETC + d] = 0.0f;
+      }
     }
     __syncthreads();
     const int nm4 = (nm + 3) >> 2;
     const int4 *sc4 = reinterpret_cast<const int4 *>(sc);
     const float4 *pr4 = reinterpret_cast<const float4 *>(prob);
-    for (int k = threadIdx.x; k < rmax; k += NT) {
-      const float *e0 = etab + ETC + (k - range);
-      float sum = 0.0f;
-      for (int m4 = 0; m4 < nm4; m4++) {
-        const int4 v = sc4[m4];
-        const float4 p = pr4[m4];
-        sum += p.x * e0[-v.x];
-        sum += p.y * e0[-v.y];
-        sum += p.z * e0[-v.z];
-        sum += p.w * e0[-v.w];
-      }
-      out[k] = sum;
+    const int lane = threadIdx.x & 31, groups = (rmax + 31) >> 5;
+    for (int g = threadIdx.x >> 5; g < groups; g += 4 * NW) {
+      const int k0 = g * 32 + lane, nc = min(4, (groups - g + NW - 1) / NW);
+      const float *e0 = etab + ETC + (k0 - range);
+      if (nc == 4)
+        noise_mix<4, NW>(e0, sc4, pr4, nm4, out, k0, rmax);
+      else if (nc == 3)
+        noise_mix<3, NW>(e0, sc4, pr4, nm4, out, k0, rmax);
+      else if (nc == 2)
+        noise_mix<2, NW>(e0, sc4, pr4, nm4, out, k0, rmax);
+      else
+        noise_mix<1, NW>(e0, sc4, pr4, nm4, out, k0, rmax);
     }
     return;
   }
@@ -1523,9 +1560,19 @@ cudaError_t launch_frame_prep(FrameDev *fr, int nf, int w, int h, cudaStream_t s
 
 // A batch whose frames have no WZ block (every block intra or skipped) has
 // max_nsir == 0: the per-WZ-block kernels have nothing to do and are not launched.
-cudaError_t launch_noise_dist(FrameDev *fr, int nf, int max_nsir, const XlmDev &xt, int band, cudaStream_t s) {
+// The block has about one warp per 128 values of the widest pdf of the band
+// (2 * max_range + 1 values), so that each lane sums up to four of them.
+cudaError_t launch_noise_dist(FrameDev *fr, int nf, int max_nsir, const XlmDev &xt, int band, int max_range,
+                              cudaStream_t s) {
   if (max_nsir <= 0) return cudaSuccess;
-  noise_dist_kernel<256><<<dim3(max_nsir, nf), 256, 0, s>>>(fr, xt, band);
+  const dim3 grid(max_nsir, nf);
+  const int warps = (2 * max_range + 1 + 127) / 128;
+  if (warps <= 2)
+    noise_dist_kernel<64><<<grid, 64, 0, s>>>(fr, xt, band);
+  else if (warps <= 4)
+    noise_dist_kernel<128><<<grid, 128, 0, s>>>(fr, xt, band);
+  else
+    noise_dist_kernel<256><<<grid, 256, 0, s>>>(fr, xt, band);
   return cudaGetLastError();
 }
 
