@@ -865,6 +865,47 @@ __global__ void __launch_bounds__(NT) noise_dist_kernel(FrameDev *frames, XlmDev
   }
 }
 
+// p[lo0..hi0) and p[lo1..hi1), each summed in ascending order (the float sums
+// of condBitProb).  The rows are read 16 bytes at a time once aligned, and
+// the two chains advance together, so two additions are in flight.
+__device__ __forceinline__ void interval_sums(const float *p, int lo0, int hi0, int lo1, int hi1, float &s0,
+                                              float &s1) {
+  float a = 0.0f, b = 0.0f;
+  int q0 = lo0, q1 = lo1;
+  for (; q0 < hi0 && (reinterpret_cast<uintptr_t>(p + q0) & 15); q0++) a += __ldg(p + q0);
+  for (; q1 < hi1 && (reinterpret_cast<uintptr_t>(p + q1) & 15); q1++) b += __ldg(p + q1);
+  for (; q0 + 4 <= hi0 && q1 + 4 <= hi1; q0 += 4, q1 += 4) {
+    const float4 u = __ldg(reinterpret_cast<const float4 *>(p + q0));
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(p + q1));
+    a += u.x;
+    b += v.x;
+    a += u.y;
+    b += v.y;
+    a += u.z;
+    b += v.z;
+    a += u.w;
+    b += v.w;
+  }
+  for (; q0 + 4 <= hi0; q0 += 4) {
+    const float4 u = __ldg(reinterpret_cast<const float4 *>(p + q0));
+    a += u.x;
+    a += u.y;
+    a += u.z;
+    a += u.w;
+  }
+  for (; q1 + 4 <= hi1; q1 += 4) {
+    const float4 v = __ldg(reinterpret_cast<const float4 *>(p + q1));
+    b += v.x;
+    b += v.y;
+    b += v.z;
+    b += v.w;
+  }
+  for (; q0 < hi0; q0++) a += __ldg(p + q0);
+  for (; q1 < hi1; q1++) b += __ldg(p + q1);
+  s0 = a;
+  s1 = b;
+}
+
 // condBitProb, noiseModel.cpp:191-310: LR = p0/p1 from sequential interval
 // sums of the pdf, one thread per 4x4 block.  Non-WZ blocks get the
 // reference's certain-zero ratio when the frame has skip or intra blocks.
@@ -890,8 +931,7 @@ __global__ void cond_bit_kernel(FrameDev *frames, int band, int bit) {
     const int b0l = rc << bit, b1l = ((rc << 1) + 1) << (bit - 1);
     const int b0u = b0l + iq, b1u = b1l + iq;
     const int v0l = b0l * step, v1l = b1l * step, v0u = (b0u + 1) * step, v1u = (b1u + 1) * step;
-    for (int q = max(v0l, 0); q < min(v0u, range); q++) p0 += p[q];
-    for (int q = max(v1l, 0); q < min(v1u, range); q++) p1 += p[q];
+    interval_sums(p, max(v0l, 0), min(v0u, range), max(v1l, 0), min(v1u, range), p0, p1);
   } else {
     const int ls = F.level_shift[index];
     const int b0l = (rc << bit) - ls;
@@ -904,8 +944,7 @@ __global__ void cond_bit_kernel(FrameDev *frames, int band, int bit) {
     const int v0u = ((b0u < 0) ? b0u * step + 1 : (b0u + 1) * step) + range;
     const int v1u = ((b1u < 0) ? b1u * step + 1 : (b1u + 1) * step) + range;
     const int len = 2 * range + 1;
-    for (int q = max(v0l + range, 0); q < min(v0u, len); q++) p0 += p[q];
-    for (int q = max(v1l + range, 0); q < min(v1u, len); q++) p1 += p[q];
+    interval_sums(p, max(v0l + range, 0), min(v0u, len), max(v1l + range, 0), min(v1u, len), p0, p1);
   }
   p0 = p0 / (p0 + p1);
   p1 = 1 - p0;
@@ -1251,7 +1290,19 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
 
 // ------------------------------------------------------ motion learning
 
-// updateSMF, motionLearning.cpp:70-127: one warp per WZ block
+// bytes a[0..3], the first lowest, from the aligned words that hold them
+__device__ __forceinline__ uint32_t load4_u8(const uint8_t *a) {
+  const uintptr_t u = reinterpret_cast<uintptr_t>(a);
+  const uint32_t *wp = reinterpret_cast<const uint32_t *>(u & ~(uintptr_t)3);
+  const uint32_t sh = (uint32_t)(u & 3) * 8;
+  const uint32_t lo = wp[0], hi = sh ? wp[1] : 0u;
+  return __funnelshift_r(lo, hi, sh);
+}
+
+// updateSMF, motionLearning.cpp:70-127: one warp per WZ block.  The block's
+// float sum of squared pixel differences only ever holds integers below 2^24
+// (16 terms of at most 255^2), so every float step of it is exact and it
+// equals the integer sum, taken here four pixels at a time (vabsdiffu4, dp4a).
 __global__ void update_smf_kernel(FrameDev *frames, XlmDev xt, int band) {
   FrameDev &F = frames[blockIdx.y];
   if (!F.active || !in_step(F, band, 0)) return;
@@ -1264,19 +1315,22 @@ __global__ void update_smf_kernel(FrameDev *frames, XlmDev xt, int band) {
   const int cw = wn.sr - wn.sl + 1, nc = cw * (wn.sb - wn.st + 1);
   const XlSmall xs = xl_small_global(xt);
   float *p = F.smf + (size_t)warp * ML_N;
+  uint32_t cb[4];
+#pragma unroll
+  for (int ii = 0; ii < 4; ii++) cb[ii] = load4_u8(F.recon + (size_t)(top + ii) * w + left);
   float pr[3];
   for (int r = 0; r < 3; r++) {
     const int q = lane + 32 * r;
     pr[r] = 0.0f;
     if (q < nc) {
       const int m = wn.st + q / cw, n = wn.sl + q % cw;
-      float sse = 0.0f;
-      for (int ii = 0; ii < 4; ii++)
-        for (int jj = 0; jj < 4; jj++) {
-          const float d = (float)F.recon[(top + ii) * w + left + jj] - (float)F.si[(m + ii) * w + n + jj];
-          sse += d * d;
-        }
-      pr[r] = xl_expf(xt, xs, (float)-0.01f * sse);
+      uint32_t sse = 0;
+#pragma unroll
+      for (int ii = 0; ii < 4; ii++) {
+        const uint32_t d = __vabsdiffu4(cb[ii], load4_u8(F.si + (size_t)(m + ii) * w + n));
+        sse = __dp4a(d, d, sse);
+      }
+      pr[r] = xl_expf(xt, xs, (float)-0.01f * (float)sse);
     }
   }
   // sequential sum in candidate order
