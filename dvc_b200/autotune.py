@@ -11,7 +11,7 @@ Five launch parameters are chosen by measurement on the device the tuner runs on
     is decoded by max(floor, SMs / codewords in flight) blocks, each starting at
     another code of the ladder (1 turns speculation off);
   - threads per updateSI search block, 64, 128 or 256 (one block per WZ 4x4
-    block: 2 x 65 candidate columns over the threads);
+    block: 2 x 65 candidate columns, two adjacent ones per thread);
   - threads per forward-search block, 128, 256 or 512 (one block per 16x16
     macroblock: 65 x 65 candidate positions over the threads).
 The search is coordinate-wise: starting from the library's defaults, each
@@ -37,7 +37,7 @@ import numpy as np
 ENV_THREADS, ENV_THREADS_QCIF, ENV_FLOOR = "DVC_LDPCA_THREADS", "DVC_LDPCA_THREADS_QCIF", "DVC_LDPCA_SPEC_FLOOR"
 ENV_SI, ENV_FME = "DVC_SI_THREADS", "DVC_FME_THREADS"
 KNOBS = [(ENV_THREADS, ("1024", "512")), (ENV_THREADS_QCIF, ("1024", "256", "512")),
-         (ENV_FLOOR, ("4", "1", "2", "8", "12", "16", "24", "32")), (ENV_SI, ("128", "64", "256")),
+         (ENV_FLOOR, ("4", "1", "2", "8", "12", "16", "24", "32")), (ENV_SI, ("64", "128", "256")),
          (ENV_FME, ("256", "128", "512"))]
 ENV_ALL = tuple(k for k, _ in KNOBS)
 THREADS = ("1024", "512")

@@ -68,7 +68,7 @@ bool Context::init(const char *data, const char *tables, int dev) {
   // the same for the motion searches: threads per updateSI and forward-search block
   const char *si = getenv("DVC_SI_THREADS");
   const char *fme = getenv("DVC_FME_THREADS");
-  set_me_shapes(si ? atoi(si) : 128, fme ? atoi(fme) : 256);
+  set_me_shapes(si ? atoi(si) : 64, fme ? atoi(fme) : 256);
 
   // library-exact math tables: load, or sweep the C library once and cache
   const std::string xpath = table_dir + "/xlm_tables.bin";

@@ -1095,7 +1095,7 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
               ((uint32_t)cur[4 * m + 3] << 24);
   }
   __syncthreads();
-  // one thread per (reference, candidate column): the SAD of candidate row yo
+  // each thread walks candidate columns of one reference: the SAD of candidate row yo
   // is the sum over m of the 4-pixel SAD of window row yo + m against block
   // row m, accumulated while walking the window rows once.  The weight is at
   // least 1, so cost = sad * weight >= sad (rounding is monotone): a candidate
@@ -1141,34 +1141,41 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     if (i2 >= 0) better(bp, ip, c2, i2);
     if (i3 >= 0) better(bf, jf, c3, i3);
   }
-  // whole columns for every thread; when at most two columns are past the
-  // last multiple of NT (2 of the 130 of an interior block at NT = 64 or
-  // 128) they go candidate by candidate below instead of costing one more
-  // pass for a couple of lanes
-  const int ncol = 2 * cw, nstream = (ncol > NT && ncol % NT <= 2) ? ncol - ncol % NT : ncol;
-  for (int pc = threadIdx.x; pc < nstream; pc += NT) {
-    const bool fut = pc >= cw;
-    const int xo = fut ? pc - cw : pc;
+  // two adjacent candidate columns (xo, xo + 1) of one reference per thread:
+  // one row read (two words) serves both, and one vote per four rows covers
+  // the eight candidates they complete.  With an odd number of columns the
+  // last column of each reference goes candidate by candidate below.
+  const int np = cw >> 1;
+  for (int pi = threadIdx.x; pi < 2 * np; pi += NT) {
+    const bool fut = pi >= np;
+    const int xo = 2 * (fut ? pi - np : pi);
     const uint8_t *wb = fut ? wf : wp;
     const uint32_t *row = reinterpret_cast<const uint32_t *>(wb) + ((xo + wo) >> 2);
     const int sh = ((xo + wo) & 3) * 8;
     const double *wt = d_si_weight + (st - top + 32) * 65 + (sl + xo - left + 32);
-    int part[4] = {0, 0, 0, 0};  // running SADs of candidate rows y-3 .. y (indexed by row & 3)
+    // running SADs of candidate rows y-3 .. y (indexed by row & 3) of both columns
+    int pa[4] = {0, 0, 0, 0}, pb[4] = {0, 0, 0, 0};
     double best = fut ? bf : bp;
     int bi = fut ? jf : ip, thr = (int)best;
     // window row y is row m of candidate y - m; candidate y - 3 is complete at row y
     auto add_row = [&](int y, int slot) {
       const uint32_t *rw = row + y * (WS / 4);
-      const uint32_t v = __funnelshift_r(rw[0], rw[1], sh);
-      part[slot & 3] = (int)sad4_acc(v, c0, 0u);
-      part[(slot - 1) & 3] = (int)sad4_acc(v, c1, (uint32_t)part[(slot - 1) & 3]);
-      part[(slot - 2) & 3] = (int)sad4_acc(v, c2, (uint32_t)part[(slot - 2) & 3]);
-      part[(slot - 3) & 3] = (int)sad4_acc(v, c3, (uint32_t)part[(slot - 3) & 3]);
+      const uint32_t lo = rw[0], hi = rw[1];
+      const uint32_t va = __funnelshift_r(lo, hi, sh), vb = __funnelshift_rc(lo, hi, sh + 8);
+      pa[slot & 3] = (int)sad4_acc(va, c0, 0u);
+      pb[slot & 3] = (int)sad4_acc(vb, c0, 0u);
+      pa[(slot - 1) & 3] = (int)sad4_acc(va, c1, (uint32_t)pa[(slot - 1) & 3]);
+      pb[(slot - 1) & 3] = (int)sad4_acc(vb, c1, (uint32_t)pb[(slot - 1) & 3]);
+      pa[(slot - 2) & 3] = (int)sad4_acc(va, c2, (uint32_t)pa[(slot - 2) & 3]);
+      pb[(slot - 2) & 3] = (int)sad4_acc(vb, c2, (uint32_t)pb[(slot - 2) & 3]);
+      pa[(slot - 3) & 3] = (int)sad4_acc(va, c3, (uint32_t)pa[(slot - 3) & 3]);
+      pb[(slot - 3) & 3] = (int)sad4_acc(vb, c3, (uint32_t)pb[(slot - 3) & 3]);
     };
-    auto weigh = [&](int yo, int sad) {
+    // column xo + xc, candidate row yo
+    auto weigh = [&](int yo, int xc, int sad) {
       if (sad <= thr) {
-        const double cst = (double)sad * __ldg(wt + yo * 65);
-        const int idx = yo * cw + xo;
+        const double cst = (double)sad * __ldg(wt + yo * 65 + xc);
+        const int idx = yo * cw + xo + xc;
         if (cst < 10000000.0 && (cst < best || (cst == best && idx < bi))) {
           best = cst;
           bi = idx;
@@ -1181,55 +1188,65 @@ __global__ void __launch_bounds__(NT) update_si_kernel(FrameDev *frames, int ban
     add_row(1, 1);
     add_row(2, 2);
     int y = 3;
-    // slots of rows y .. y+3 are 3, 0, 1, 2 (y = 3 mod 4); the four candidates
-    // completed by a group are weighed after it, in order, and only when one
-    // lane of the warp has one that can match its best (the lanes run the same
-    // rows, so the vote is taken by the whole active warp): a warp branches
-    // once per four rows, and rarely
+    // slots of rows y .. y+3 are 3, 0, 1, 2 (y = 3 mod 4); the candidates
+    // completed by a group are weighed after it, and only when one lane of the
+    // warp has one that can match its best (the lanes run the same rows, so
+    // the vote is taken by the whole active warp): a warp branches once per
+    // four rows, and rarely.  The (cost, index) order makes the result
+    // independent of the order in which candidates are weighed.
     for (; y + 3 < wh; y += 4) {
-      int sd[4];
+      int sa[4], sb[4];
 #pragma unroll
       for (int r = 0; r < 4; r++) {
         add_row(y + r, 3 + r);
-        sd[r] = part[r & 3];
+        sa[r] = pa[r & 3];
+        sb[r] = pb[r & 3];
       }
-      if (__any_sync(__activemask(), min(min(sd[0], sd[1]), min(sd[2], sd[3])) <= thr)) {
+      const int mn = min(min(min(sa[0], sa[1]), min(sa[2], sa[3])), min(min(sb[0], sb[1]), min(sb[2], sb[3])));
+      if (__any_sync(__activemask(), mn <= thr)) {
 #pragma unroll
-        for (int r = 0; r < 4; r++) weigh(y + r - 3, sd[r]);
+        for (int r = 0; r < 4; r++) {
+          weigh(y + r - 3, 0, sa[r]);
+          weigh(y + r - 3, 1, sb[r]);
+        }
       }
     }
     for (; y < wh; y++) {  // the last rows; y - 3 mod 4 as above
       const uint32_t *rw = row + y * (WS / 4);
-      const uint32_t v = __funnelshift_r(rw[0], rw[1], sh);
+      const uint32_t lo = rw[0], hi = rw[1];
       const int q = y & 3;
-      // the same updates with the slot of row y known only at run time
-      int p0 = part[0], p1 = part[1], p2 = part[2], p3 = part[3];
-      const int s0 = (int)__vsadu4(v, c0), s1 = (int)__vsadu4(v, c1), s2 = (int)__vsadu4(v, c2),
-                s3 = (int)__vsadu4(v, c3);
-      // slot q gets s0 (new), q-1 += s1, q-2 += s2, q-3 (= q+1) += s3
-      int n[4] = {p0, p1, p2, p3};
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const int d = (q - k) & 3;  // 0: new candidate, 1..3: candidates started 1..3 rows ago
-        n[k] = d == 0 ? s0 : d == 1 ? n[k] + s1 : d == 2 ? n[k] + s2 : n[k] + s3;
-      }
-      part[0] = n[0];
-      part[1] = n[1];
-      part[2] = n[2];
-      part[3] = n[3];
       const int done = (q + 1) & 3;  // slot of candidate y - 3
-      weigh(y - 3, done == 0 ? part[0] : done == 1 ? part[1] : done == 2 ? part[2] : part[3]);
+      // the same updates with the slot of row y known only at run time:
+      // slot q gets the new candidate, q-1 += row 1, q-2 += row 2, q-3 (= q+1) += row 3
+#pragma unroll
+      for (int xc = 0; xc < 2; xc++) {
+        const uint32_t v = xc ? __funnelshift_rc(lo, hi, sh + 8) : __funnelshift_r(lo, hi, sh);
+        int *part = xc ? pb : pa;
+        const int s0 = (int)__vsadu4(v, c0), s1 = (int)__vsadu4(v, c1), s2 = (int)__vsadu4(v, c2),
+                  s3 = (int)__vsadu4(v, c3);
+        int n[4] = {part[0], part[1], part[2], part[3]};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int d = (q - k) & 3;  // 0: new candidate, 1..3: candidates started 1..3 rows ago
+          n[k] = d == 0 ? s0 : d == 1 ? n[k] + s1 : d == 2 ? n[k] + s2 : n[k] + s3;
+        }
+        part[0] = n[0];
+        part[1] = n[1];
+        part[2] = n[2];
+        part[3] = n[3];
+        weigh(y - 3, xc, done == 0 ? n[0] : done == 1 ? n[1] : done == 2 ? n[2] : n[3]);
+      }
     }
     if (fut) better(bf, jf, best, bi);
     else better(bp, ip, best, bi);
   }
-  {
-    // at most two columns remain: the column of candidate k is k >= nrow
-    const int nrow = wh - 3, nrest = ncol - nstream;
-    for (int k = threadIdx.x; k < nrest * nrow; k += NT) {
-      const int hi = k >= nrow, pc = nstream + hi, yo = k - hi * nrow;
-      const bool fut = pc >= cw;
-      const int xo = fut ? pc - cw : pc;
+  if (cw & 1) {
+    // the last column (cw - 1) of each reference: candidate k of the past
+    // window's column for k < nrow, of the future window's above
+    const int nrow = wh - 3, xo = cw - 1;
+    for (int k = threadIdx.x; k < 2 * nrow; k += NT) {
+      const bool fut = k >= nrow;
+      const int yo = k - (fut ? nrow : 0);
       const int sad = sad_at(fut ? wf : wp, yo, xo);
       const double cst = (double)sad * __ldg(d_si_weight + (st - top + 32 + yo) * 65 + (sl + xo - left + 32));
       if (cst < 10000000.0) {
@@ -1576,10 +1593,10 @@ static inline dim3 g2(int n, int tpb, int frames) { return dim3((n + tpb - 1) / 
 // threads per search block of the two motion searches (the candidate columns
 // or positions each thread walks follow from it); process-wide, set when a
 // context is created (dvc_b200.autotune picks them; the output never depends on them)
-static int g_si_threads = 128, g_fme_threads = 256;
+static int g_si_threads = 64, g_fme_threads = 256;
 
 void set_me_shapes(int si_threads, int fme_threads) {
-  g_si_threads = (si_threads == 64 || si_threads == 256) ? si_threads : 128;
+  g_si_threads = (si_threads == 128 || si_threads == 256) ? si_threads : 64;
   g_fme_threads = (fme_threads == 128 || fme_threads == 512) ? fme_threads : 256;
 }
 
